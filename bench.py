@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Throughput of the weighted alpha complex engine on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (per rank): a 100,000-ball synthetic globule (self-avoiding walk,
+0.05 balls/A^3, C/N/O/S radii), solvent radius 1.4, alpha 1.0, upstream
+formulas, the empty-orthosphere test applied (as the reference source is
+written), strict single-precision arithmetic.  A step is one full pass: balls
+in, the sorted edge/triangle/tetrahedron lists out.  Every rank builds its
+own molecule (seeded by rank): the work partitions with no collective, so
+scaling is weak.
+
+Prints one JSON line (rank 0).  `value` is device-resident throughput
+(inputs already in HBM, lists left in HBM); `e2e` goes through the host C ABI
+(pac_alpha_complex: host balls in, pinned host lists out, copies inside the
+timed region).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as ge  # noqa: E402
+
+N_BALLS = 100_000
+SOL, ALPHA = 1.4, 1.0
+METRIC = "balls/s to bit-exact alpha complex at 100k balls"
+CPU_SAMPLE = 10_000
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the tetrahedron kernel from the committed ncu
+    summary (profiles/k_tets_*.md, line 'traffic_bytes_per_launch_full: X')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if f.startswith("k_tets") and f.endswith(".md"):
+            for line in open(os.path.join(d, f)):
+                if line.strip().startswith("traffic_bytes_per_launch_full:"):
+                    try:
+                        return float(line.split(":", 1)[1].strip().split()[0])
+                    except ValueError:
+                        return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:
+            pass
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+            os.unlink(self.path)
+        except Exception:
+            return None
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(threads):
+    """The CPU restatement (OpenMP, all host threads) on a bounded sample of
+    the same workload: a 10,000-ball globule, same sol-rad/alpha/formulas."""
+    pac = ge.load_package()
+    orc = ge.load_oracle()
+    balls = pac.globule(CPU_SAMPLE, seed=pac.SEED_BASE + 4)
+    t0 = time.perf_counter()
+    orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": CPU_SAMPLE / dt, "unit": "balls/s", "cores": threads, "kind": "port",
+            "sample": "%d-ball globule, sol 1.4, alpha 1.0, as-written, %.2f s" % (CPU_SAMPLE, dt)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    pac = ge.load_package()
+    orc = ge.load_oracle()
+    balls = pac.globule(CPU_SAMPLE, seed=pac.SEED_BASE + 4)
+    for _ in range(max(args.warmup, 0) and 1):
+        orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
+        t.append(time.perf_counter() - t0)
+    per = sum(t) / len(t)
+    v = CPU_SAMPLE / per
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "balls/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "globule, sol 1.4, alpha 1.0 (CPU sample of %d balls)" % CPU_SAMPLE,
+                       "n_balls": CPU_SAMPLE, "sol_rad": SOL, "alpha": ALPHA},
+            "cpu_baseline": {"value": v, "unit": "balls/s", "cores": threads, "kind": "port",
+                             "sample": "%d-ball globule per step" % CPU_SAMPLE},
+            "e2e": {"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_BALLS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    pac = ge.load_package()
+    n = args.n
+    balls = pac.globule(n, seed=pac.SEED_BASE + 4 + 1000 * rank)
+    eng = pac.Engine(device=local, formula="upstream", tet_mode="as-written", predicates="strict")
+    d_balls = torch.from_numpy(balls).cuda()
+    stream = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        cx, st = eng.alpha_complex_device(d_balls.data_ptr(), n, SOL, ALPHA)
+
+    # ---- device-resident timed region
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stats = []
+    sampler = ClockSampler(local)
+    barrier()
+    with sampler:
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev[k][0].record(stream)
+            cx, st = eng.alpha_complex_device(d_balls.data_ptr(), n, SOL, ALPHA)
+            ev[k][1].record(stream)
+            stats.append(st)
+        barrier()
+        wall = time.perf_counter() - t0
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_max = dev_ms
+    if dist:
+        t = torch.tensor([dev_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    ms_per_step = t_max / args.steps
+    value = world * n / (ms_per_step / 1e3)
+
+    # ---- end-to-end through the host C ABI
+    e2e_ms = []
+    h2d = d2h = 0
+    eng.alpha_complex(balls, SOL, ALPHA)
+    barrier()
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r = eng.alpha_complex(balls, SOL, ALPHA)
+        e2e_ms.append(max(r.stats["ms_total"], 0.0))
+        e2e_wall = time.perf_counter() - t1
+        h2d = balls.nbytes
+        d2h = r.edges.nbytes + r.tris.nbytes + r.tets.nbytes
+    e2e_step = sum(e2e_ms) / len(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    e2e_value = world * n / (e2e_step / 1e3)
+
+    # ---- roofline of the dominant kernel (fused tetrahedron pass)
+    s0 = stats[-1]
+    tet_ms = sum(s["ms_tets"] for s in stats) / len(stats)
+    # reference byte model: every candidate tetrahedron (16 B) and its
+    # orthosphere (16 B) written once and read once
+    alg_bytes = 64.0 * s0["cand_tets"]
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (tet_ms / 1e3) / 1e9
+    traffic = profiled_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(os.cpu_count() or 1)
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    clocks = sampler.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "balls/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "100k-ball globule (0.05/A^3), sol 1.4, alpha 1.0, upstream "
+                               "formulas, orthosphere test applied, strict f32",
+                   "n_balls": n, "sol_rad": SOL, "alpha": ALPHA, "parallelism": "dp%d" % world,
+                   "l2": "flushed between steps (256 MB write)"},
+        "simplices_per_s": world * (s0["final_edges"] + s0["final_tris"] + s0["final_tets"] + n)
+        / (ms_per_step / 1e3),
+        "complex": {"edges": s0["final_edges"], "tris": s0["final_tris"], "tets": s0["final_tets"],
+                    "cand_tets": s0["cand_tets"], "alpha_tets": s0["alpha_tets"],
+                    "insphere_evals": s0["insphere_evals"], "sos_calls": s0["sos_calls"]},
+        "stage_ms": {k: s0[k] for k in ("ms_grid", "ms_edges", "ms_tris", "ms_tets",
+                                        "ms_tri_attach", "ms_edge_attach", "ms_emit")},
+        "e2e": {"value": e2e_value, "unit": "balls/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_tets (fused enumeration + alpha + orthosphere)",
+                     "bytes_model": "64 B x candidate tetrahedra", "kernel_ms": tet_ms},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(sum(s["kernels_launched"] for s in stats)),
+        "clocks": clocks,
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

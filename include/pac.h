@@ -1,0 +1,216 @@
+/*
+ * pac.h -- C ABI of the B200 weighted alpha complex engine (libpac.so).
+ *
+ * The reference (forest113/ParallelAC-xmp) has no library interface: its
+ * only boundary is the process CLI
+ *     parallelac <crd> <out> <sol-rad> <alpha>              (AlphaComplexParallel.cu:1053-1057)
+ *     parallelac-largeData <crd> <out> <sol-rad> <alpha> <chunk-size>
+ *                                                           (AlphaComplexLargeData.cu:1049-1058)
+ * and each main() runs the whole pipeline inline.  The entry points below
+ * are what an FFI (ctypes, cgo, JNI) binds to run that same pipeline without
+ * the process boundary; the two CLIs shipped with this library are thin
+ * callers of them.  Each declaration names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every entry point returns a pac_status (0 = PAC_OK, negative = error)
+ *     and never exits the process.
+ *   - A pac_ctx owns one CUDA stream and a device memory pool; it is not
+ *     thread-safe.  Use one context per host thread.
+ *   - Balls are float4 (x, y, z, raw radius) in input order; the solvent
+ *     radius is added on the device (AlphaComplexLargeData.cu:1085).
+ *   - Output vertex indices are 0-based input indices.  With
+ *     PAC_ORDER_REFERENCE the lists come in the reference binary's file order
+ *     (AlphaComplexLargeData.cu:2036-2050); with PAC_ORDER_CANONICAL every
+ *     simplex is sorted ascending and each list is sorted lexicographically.
+ */
+#ifndef PAC_H
+#define PAC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PAC_ABI_VERSION 1
+
+typedef enum {
+    PAC_OK = 0,
+    PAC_ERR_INVALID_ARG = -1, /* null pointer, NaN/inf input, bad option */
+    PAC_ERR_CUDA = -2,        /* a CUDA call failed; see pac_last_error() */
+    PAC_ERR_CAPACITY = -3,    /* an internal limit was exceeded (e.g. degree) */
+    PAC_ERR_TIMEOUT = -4,     /* a bounded device wait gave up */
+    PAC_ERR_NO_DEVICE = -5,   /* no CUDA device / extension not usable */
+    PAC_ERR_EXACT_RANGE = -6, /* exact arithmetic width exceeded */
+    PAC_ERR_OOM = -7,         /* device or host allocation failed */
+    PAC_ERR_IO = -8           /* file could not be read or written */
+} pac_status;
+
+/* Which of the reference's two formula sets the filters use. */
+typedef enum {
+    /* AlphaComplexLargeData.cu:167-190, 298-348 (binary parallelac-largeData) */
+    PAC_FORMULA_UPSTREAM = 0,
+    /* AlphaComplexParallel.cu:203-230, 310-372 (binary parallelac), including
+       its division-free edge test and its triangle right-hand side
+       `a31*x + a32*y + a33*z*2` (AlphaComplexParallel.cu:344) */
+    PAC_FORMULA_PLAIN_XMP = 1
+} pac_formula;
+
+/* The empty-orthosphere test of the alpha tetrahedra
+   (checkTetsOrthosphere, AlphaComplexLargeData.cu:597-735). */
+typedef enum {
+    /* Apply it, as the source is written.  This is the weighted alpha
+       complex proper. */
+    PAC_TETS_AS_WRITTEN = 0,
+    /* Skip it, as the reference binary behaves: checkTetsOrthosphere needs
+       161 registers per thread for sm_100a and is launched with 512-thread
+       blocks (AlphaComplexLargeData.cu:1158, 1492), the launch fails with
+       "too many resources requested", the error is only printed
+       (AlphaComplexLargeData.cu:51-57), and every alpha-filtered tetrahedron
+       is kept.  The shipped golden outputs were produced this way. */
+    PAC_TETS_AS_RUN = 1
+} pac_tet_mode;
+
+/* Arithmetic of the predicates. */
+typedef enum {
+    /* Single-precision operations in the reference's order, without FMA
+       contraction (= the reference built with nvcc -fmad=false); exact
+       simulation of simplicity on an insphere result of exactly zero
+       (predicates.h:4669-5462). */
+    PAC_PRED_REFCOMPAT = 0,
+    /* Same, but every operation that the reference leaves to nvcc's default
+       FMA contraction is compiled with contraction enabled (nvcc -fmad=true),
+       to follow the reference binary built with default flags. */
+    PAC_PRED_REFCOMPAT_FMA = 1,
+    /* Exact decisions: a double-precision semi-static filter for each
+       orientation/power/attachment test and an exact multi-word integer
+       evaluation for the cases the filter cannot decide. */
+    PAC_PRED_EXACT = 2
+} pac_pred_mode;
+
+typedef enum { PAC_ORDER_REFERENCE = 0, PAC_ORDER_CANONICAL = 1 } pac_order;
+
+typedef struct {
+    int device;      /* CUDA device ordinal, default 0 */
+    int formula;     /* pac_formula, default PAC_FORMULA_UPSTREAM */
+    int tet_mode;    /* pac_tet_mode, default PAC_TETS_AS_WRITTEN */
+    int predicates;  /* pac_pred_mode, default PAC_PRED_REFCOMPAT */
+    int order;       /* pac_order, default PAC_ORDER_REFERENCE */
+    int autotune;    /* 1: pick launch shapes by measurement (batched mode) */
+    int verbose;     /* 1: print per-stage timings to stderr */
+    int reserved_i[9];
+    uint64_t reserved_u[8];
+} pac_options;
+
+typedef struct {
+    float x, y, z, r;
+} pac_ball;
+
+/* One complex.  Lists are owned by the library and released with
+   pac_free_complex().  on_device = 1 means the three pointers are device
+   pointers (from pac_alpha_complex_device). */
+typedef struct {
+    uint32_t n_vertices;
+    uint32_t on_device;
+    uint64_t n_edges, n_tris, n_tets;
+    uint32_t *edges; /* 2 * n_edges */
+    uint32_t *tris;  /* 3 * n_tris */
+    uint32_t *tets;  /* 4 * n_tets */
+} pac_complex;
+
+/* Many molecules: the lists of molecule m are rows [off[m], off[m+1]) of
+   the concatenated lists, with molecule-local vertex indices. */
+typedef struct {
+    uint32_t n_mol;
+    uint32_t on_device;
+    uint64_t *edge_off, *tri_off, *tet_off; /* n_mol + 1 each (host) */
+    uint32_t *edges, *tris, *tets;
+} pac_batch_complex;
+
+/* Stage counters and timings (filled when a non-null pointer is passed). */
+typedef struct {
+    uint64_t n_balls, n_cells;
+    uint64_t cand_edges, alpha_edges;
+    uint64_t cand_tris, alpha_tris;
+    uint64_t cand_tets, alpha_tets;
+    uint64_t final_edges, final_tris, final_tets;
+    uint64_t insphere_evals;  /* insphere_w evaluations (as-written mode) */
+    uint64_t sos_calls;       /* insphere results of exactly 0 -> SoS */
+    uint64_t exact_fallbacks; /* exact-mode: filter failures -> exact kernel */
+    uint64_t filter_evals;    /* exact-mode: filtered decisions */
+    uint64_t ortho_out_of_grid; /* window centres outside the grid */
+    uint64_t max_degree;
+    double ms_total, ms_h2d, ms_grid, ms_edges, ms_tris, ms_tets, ms_tri_attach,
+        ms_edge_attach, ms_emit, ms_d2h;
+    uint64_t bytes_model; /* algorithmic bytes of the pass */
+    uint32_t grid[3];
+    float step;
+    uint32_t kernels_launched;
+} pac_stats;
+
+/* Version of this ABI (PAC_ABI_VERSION). */
+int pac_abi_version(void);
+
+/* Defaults: device 0, upstream formulas, as-written tets, ref-compat
+   predicates, reference order. */
+void pac_default_options(pac_options *opt);
+
+/* Create / destroy a context.  Replaces the implicit CUDA context, the
+   initialize<<<1,1>>>() exactinit() launch and the Thrust allocations of
+   AlphaComplexLargeData.cu:1145-1155. */
+typedef struct pac_ctx pac_ctx;
+int pac_create(pac_ctx **ctx, const pac_options *opt);
+int pac_destroy(pac_ctx *ctx);
+
+/* The cudaStream_t (as void*) this context launches on, so a caller can
+   order its own work, or record timing events, against the engine's.  No
+   reference counterpart (the reference uses the default stream). */
+void *pac_cuda_stream(pac_ctx *ctx);
+
+/* Weighted alpha complex of one molecule, host buffers in and out.
+   Replaces the pipeline of AlphaComplexParallel.cu:1119-1807 and
+   AlphaComplexLargeData.cu:1119-2001 (grid, candidate enumeration, the
+   power/orientation/attachment filters and the set differences), run as a
+   single device pass without the chunk loop.
+   balls: n host balls; sol_rad and alpha as on the reference command line
+   (AlphaComplexLargeData.cu:1076-1077). */
+int pac_alpha_complex(pac_ctx *ctx, const pac_ball *balls, uint32_t n,
+                      float sol_rad, float alpha, pac_complex *out,
+                      pac_stats *stats);
+
+/* Same with device-resident input and output (d_balls is a device pointer;
+   out->on_device = 1).  Nothing crosses PCIe except a few counters. */
+int pac_alpha_complex_device(pac_ctx *ctx, const pac_ball *d_balls,
+                             uint32_t n, float sol_rad, float alpha,
+                             pac_complex *out, pac_stats *stats);
+
+/* Many independent molecules in one device pass.  balls holds the molecules
+   back to back; offsets has n_mol + 1 entries (offsets[0] = 0).  Replaces
+   running the reference binary once per molecule. */
+int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls,
+                            const uint64_t *offsets, uint32_t n_mol,
+                            float sol_rad, float alpha, pac_batch_complex *out,
+                            pac_stats *stats);
+
+void pac_free_complex(pac_complex *cx);
+void pac_free_batch_complex(pac_batch_complex *cx);
+
+/* Read a CRD file (count, then x y z r per line, parsed as %f).
+   Replaces AlphaComplexLargeData.cu:1067-1112.  *balls is malloc'ed. */
+int pac_read_crd(const char *path, pac_ball **balls, uint32_t *n);
+
+/* Write the reference's output file format (AlphaComplexLargeData.cu:2028-2050):
+   header "V E T Tet", V lines "%9.5lf" x4 (radius including sol_rad), then
+   the edge, triangle and tetrahedron lines with "%9d" fields. */
+int pac_write_complex(const char *path, const pac_ball *balls, uint32_t n,
+                      float sol_rad, const pac_complex *cx);
+
+const char *pac_status_string(int status);
+/* Detail of the last error on this host thread ("" if none). */
+const char *pac_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAC_H */

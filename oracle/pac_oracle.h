@@ -1,0 +1,75 @@
+/*
+ * pac_oracle.h -- CPU restatement of the ParallelAC weighted alpha complex
+ * pipeline.  TEST INFRASTRUCTURE ONLY: the tests, the smoke check and the
+ * bench's CPU-baseline leg link this library as the checker.  The product
+ * path (libpac) never calls it.
+ *
+ * The restatement follows AlphaComplexLargeData.cu (formula variant
+ * ORC_UPSTREAM) and AlphaComplexParallel.cu (variant ORC_PLAIN_XMP), with
+ * every single-precision operation performed in the reference's order and
+ * without contraction (build with -ffp-contract=off).  Exact predicates
+ * (the SoS fallback of predicates.h:4669-5462) use multi-word integers.
+ */
+#ifndef PAC_ORACLE_H
+#define PAC_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_UPSTREAM = 0, ORC_PLAIN_XMP = 1 };
+
+/* flags */
+enum {
+    /* Apply the empty-orthosphere test to the alpha tetrahedra
+       (checkTetsOrthosphere, LD:597-735) as the source is written.  Without
+       this flag the restatement follows the reference binary as it runs:
+       that kernel needs more registers than a 512-thread block can hold
+       (161 per thread for sm_100a), its launch fails, and every
+       alpha-filtered tetrahedron is kept. */
+    ORC_TET_ORTHO = 1
+};
+
+typedef struct {
+    /* final complex in the reference binary's output order, 0-based
+       original indices (AlphaComplexLargeData.cu:2036-2050) */
+    uint64_t n_edges, n_tris, n_tets;
+    uint32_t *edges; /* 2 per edge */
+    uint32_t *tris;  /* 3 per triangle */
+    uint32_t *tets;  /* 4 per tetrahedron */
+    /* stage counts */
+    uint64_t cand_edges, alpha_edges;
+    uint64_t cand_tris, alpha_tris;
+    uint64_t cand_tets, alpha_tets;
+    uint64_t tris_in_tets, edges_in_tris;
+    uint64_t insphere_evals, sos_calls, sos_exhausted;
+    uint64_t ortho_out_of_grid;
+    int32_t grid[3];
+    float step;
+    int status; /* 0 ok, <0 error */
+} orc_result;
+
+/* xyzr: n x 4 floats (x, y, z, raw radius) in input order. */
+int orc_alpha_complex(const float *xyzr, uint32_t n, float sol_rad,
+                      float alpha, int variant, int flags, int threads,
+                      orc_result *res);
+void orc_free(orc_result *res);
+
+/* Single predicates, exposed so the tests can pin them against the
+   reference's own predicates.h compiled for the host. */
+float orc_orient3d(const float *pa, const float *pb, const float *pc,
+                   const float *pd);
+float orc_insphere_w(const float *pa, const float *pb, const float *pc,
+                     const float *pd, const float *pe, float wa, float wb,
+                     float wc, float wd, float we);
+/* returns the SoS sign (+1/-1); *depth receives the SoS depth reached */
+int orc_sos4(const float *p0, const float *p1, const float *p2,
+             const float *p3, const float *p4, float w0, float w1, float w2,
+             float w3, float w4, int i0, int i1, int i2, int i3, int i4,
+             int *depth);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,118 @@
+"""ctypes binding of the CPU restatement (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by the bench's cpu_baseline leg, as the checker.  The product path never
+imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_PRED_PATH = os.path.join(HERE, "_ref", "libpredref.so")
+
+UPSTREAM, PLAIN_XMP = 0, 1
+TET_ORTHO = 1  # flag: apply the empty-orthosphere test as written
+
+
+class _Res(ctypes.Structure):
+    _fields_ = ([("n_edges", ctypes.c_uint64), ("n_tris", ctypes.c_uint64),
+                 ("n_tets", ctypes.c_uint64)] +
+                [(k, ctypes.POINTER(ctypes.c_uint32)) for k in ("edges", "tris", "tets")] +
+                [(k, ctypes.c_uint64) for k in
+                 ("cand_edges", "alpha_edges", "cand_tris", "alpha_tris", "cand_tets",
+                  "alpha_tets", "tris_in_tets", "edges_in_tris", "insphere_evals", "sos_calls",
+                  "sos_exhausted", "ortho_out_of_grid")] +
+                [("grid", ctypes.c_int32 * 3), ("step", ctypes.c_float), ("status", ctypes.c_int)])
+
+
+_LIB = None
+
+
+def build():
+    """Compile the restatement with its Makefile (gcc, -ffp-contract=off)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_alpha_complex.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(_Res)]
+        L.orc_free.argtypes = [ctypes.POINTER(_Res)]
+        f3 = ctypes.POINTER(ctypes.c_float)
+        L.orc_orient3d.restype = ctypes.c_float
+        L.orc_orient3d.argtypes = [f3] * 4
+        L.orc_insphere_w.restype = ctypes.c_float
+        L.orc_insphere_w.argtypes = [f3] * 5 + [ctypes.c_float] * 5
+        L.orc_sos4.restype = ctypes.c_int
+        L.orc_sos4.argtypes = [f3] * 5 + [ctypes.c_float] * 5 + [ctypes.c_int] * 5 + [
+            ctypes.POINTER(ctypes.c_int)]
+        _LIB = L
+    return _LIB
+
+
+def _take(ptr, count, k):
+    if count == 0:
+        return np.zeros((0, k), np.uint32)
+    return np.ctypeslib.as_array(ptr, (count * k,)).reshape(count, k).copy()
+
+
+def alpha_complex(balls, sol_rad, alpha, variant=UPSTREAM, tet_ortho=True, threads=0):
+    """Returns (edges, tris, tets, stats) in the reference binary's order."""
+    b = np.ascontiguousarray(balls, dtype=np.float32)
+    r = _Res()
+    rc = lib().orc_alpha_complex(b.ctypes.data_as(ctypes.c_void_p), len(b), float(sol_rad),
+                                 float(alpha), variant, TET_ORTHO if tet_ortho else 0, threads,
+                                 ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError("oracle failed: %d" % rc)
+    try:
+        E, T, Q = _take(r.edges, r.n_edges, 2), _take(r.tris, r.n_tris, 3), _take(r.tets, r.n_tets, 4)
+        st = {k: int(getattr(r, k)) for k in
+              ("cand_edges", "alpha_edges", "cand_tris", "alpha_tris", "cand_tets", "alpha_tets",
+               "tris_in_tets", "edges_in_tris", "insphere_evals", "sos_calls", "sos_exhausted",
+               "ortho_out_of_grid")}
+        st["grid"] = list(r.grid)
+        st["step"] = float(r.step)
+        return E, T, Q, st
+    finally:
+        lib().orc_free(ctypes.byref(r))
+
+
+def _fp(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def orient3d(pa, pb, pc, pd):
+    keep = [_fp(p) for p in (pa, pb, pc, pd)]
+    return lib().orc_orient3d(*[k[1] for k in keep])
+
+
+def insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we):
+    keep = [_fp(p) for p in (pa, pb, pc, pd, pe)]
+    return lib().orc_insphere_w(*[k[1] for k in keep], wa, wb, wc, wd, we)
+
+
+def sos4(pts, ws, idx):
+    keep = [_fp(p) for p in pts]
+    d = ctypes.c_int()
+    s = lib().orc_sos4(*[k[1] for k in keep], *[float(w) for w in ws], *[int(i) for i in idx],
+                       ctypes.byref(d))
+    return s, d.value
+
+
+def canonical(a):
+    """Sort vertices within each simplex, then the rows lexicographically."""
+    a = np.sort(np.asarray(a, dtype=np.int64), axis=1)
+    if len(a) == 0:
+        return a
+    return a[np.lexsort(a.T[::-1])]

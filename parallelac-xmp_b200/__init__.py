@@ -1,0 +1,328 @@
+"""Python binding of libpac (the B200 weighted alpha complex engine).
+
+The directory name is not a Python identifier, so load it by path::
+
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "parallelac_xmp_b200", "parallelac-xmp_b200/__init__.py")
+
+(``__graft_entry__.load_package()`` does exactly that.)
+
+Everything here is a thin ctypes layer over ``include/pac.h``; the work runs
+in ``lib/libpac.so``.  There is no Python or CPU fallback: if the library or a
+CUDA device is missing, the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpac.so")
+SYNTH_PATH = os.path.join(HERE, "lib", "libpac_synth.so")
+BIN_DIR = os.path.join(HERE, "bin")
+
+FORMULA = {"upstream": 0, "plain-xmp": 1}
+TET_MODE = {"as-written": 0, "as-run": 1}
+PREDICATES = {"strict": 0, "fma": 1, "exact": 2}
+ORDER = {"reference": 0, "canonical": 1}
+
+
+class PacError(RuntimeError):
+    def __init__(self, status, detail):
+        super().__init__("%s (%d): %s" % (_lib().pac_status_string(status).decode(), status, detail))
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("formula", ctypes.c_int), ("tet_mode", ctypes.c_int),
+                ("predicates", ctypes.c_int), ("order", ctypes.c_int), ("autotune", ctypes.c_int),
+                ("verbose", ctypes.c_int), ("reserved_i", ctypes.c_int * 9),
+                ("reserved_u", ctypes.c_uint64 * 8)]
+
+
+class Complex(ctypes.Structure):
+    _fields_ = [("n_vertices", ctypes.c_uint32), ("on_device", ctypes.c_uint32),
+                ("n_edges", ctypes.c_uint64), ("n_tris", ctypes.c_uint64),
+                ("n_tets", ctypes.c_uint64),
+                ("edges", ctypes.POINTER(ctypes.c_uint32)),
+                ("tris", ctypes.POINTER(ctypes.c_uint32)),
+                ("tets", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class BatchComplex(ctypes.Structure):
+    _fields_ = [("n_mol", ctypes.c_uint32), ("on_device", ctypes.c_uint32),
+                ("edge_off", ctypes.POINTER(ctypes.c_uint64)),
+                ("tri_off", ctypes.POINTER(ctypes.c_uint64)),
+                ("tet_off", ctypes.POINTER(ctypes.c_uint64)),
+                ("edges", ctypes.POINTER(ctypes.c_uint32)),
+                ("tris", ctypes.POINTER(ctypes.c_uint32)),
+                ("tets", ctypes.POINTER(ctypes.c_uint32))]
+
+
+_STAT_U64 = ["n_balls", "n_cells", "cand_edges", "alpha_edges", "cand_tris", "alpha_tris",
+             "cand_tets", "alpha_tets", "final_edges", "final_tris", "final_tets",
+             "insphere_evals", "sos_calls", "exact_fallbacks", "filter_evals",
+             "ortho_out_of_grid", "max_degree"]
+_STAT_F64 = ["ms_total", "ms_h2d", "ms_grid", "ms_edges", "ms_tris", "ms_tets",
+             "ms_tri_attach", "ms_edge_attach", "ms_emit", "ms_d2h"]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] +
+                [(k, ctypes.c_double) for k in _STAT_F64] +
+                [("bytes_model", ctypes.c_uint64), ("grid", ctypes.c_uint32 * 3),
+                 ("step", ctypes.c_float), ("kernels_launched", ctypes.c_uint32)])
+
+    def as_dict(self):
+        d = {k: int(getattr(self, k)) for k in _STAT_U64}
+        d.update({k: float(getattr(self, k)) for k in _STAT_F64})
+        d["grid"] = list(self.grid)
+        d["step"] = float(self.step)
+        d["kernels_launched"] = int(self.kernels_launched)
+        return d
+
+
+_LIB = None
+_SYNTH = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libpac.so is not built (%s); run parallelac-xmp_b200/build.py"
+                               % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.pac_status_string.restype = ctypes.c_char_p
+        L.pac_status_string.argtypes = [ctypes.c_int]
+        L.pac_last_error.restype = ctypes.c_char_p
+        L.pac_abi_version.restype = ctypes.c_int
+        L.pac_default_options.argtypes = [ctypes.POINTER(Options)]
+        L.pac_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(Options)]
+        L.pac_destroy.argtypes = [P]
+        L.pac_alpha_complex.argtypes = [P, P, ctypes.c_uint32, ctypes.c_float, ctypes.c_float,
+                                        ctypes.POINTER(Complex), ctypes.POINTER(Stats)]
+        L.pac_alpha_complex_device.argtypes = L.pac_alpha_complex.argtypes
+        L.pac_alpha_complex_batch.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_float,
+                                              ctypes.c_float, ctypes.POINTER(BatchComplex),
+                                              ctypes.POINTER(Stats)]
+        L.pac_cuda_stream.restype = ctypes.c_void_p
+        L.pac_cuda_stream.argtypes = [P]
+        L.pac_free_complex.argtypes = [ctypes.POINTER(Complex)]
+        L.pac_free_batch_complex.argtypes = [ctypes.POINTER(BatchComplex)]
+        L.pac_read_crd.argtypes = [ctypes.c_char_p, ctypes.POINTER(P),
+                                   ctypes.POINTER(ctypes.c_uint32)]
+        L.pac_write_complex.argtypes = [ctypes.c_char_p, P, ctypes.c_uint32, ctypes.c_float,
+                                        ctypes.POINTER(Complex)]
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    """The loaded libpac.so (ctypes.CDLL)."""
+    return _lib()
+
+
+def _check(status):
+    if status != 0:
+        raise PacError(status, _lib().pac_last_error().decode())
+
+
+def _arr(ptr, count, k):
+    if count == 0:
+        return np.zeros((0, k), np.uint32)
+    return np.ctypeslib.as_array(ptr, (count * k,)).reshape(count, k).copy()
+
+
+class Result:
+    """One complex: edges (E,2), tris (T,3), tets (Q,4) uint32 arrays of
+    0-based input indices, plus the stage counters of the pass."""
+
+    def __init__(self, edges, tris, tets, stats):
+        self.edges, self.tris, self.tets, self.stats = edges, tris, tets, stats
+
+    def counts(self):
+        return len(self.edges), len(self.tris), len(self.tets)
+
+
+class Engine:
+    """A pac_ctx: one CUDA stream and device memory pool on one device."""
+
+    def __init__(self, device=0, formula="upstream", tet_mode="as-written", predicates="strict",
+                 order="reference", verbose=False):
+        L = _lib()
+        o = Options()
+        L.pac_default_options(ctypes.byref(o))
+        o.device = device
+        o.formula = FORMULA[formula]
+        o.tet_mode = TET_MODE[tet_mode]
+        o.predicates = PREDICATES[predicates]
+        o.order = ORDER[order]
+        o.verbose = int(verbose)
+        self._ctx = ctypes.c_void_p()
+        _check(L.pac_create(ctypes.byref(self._ctx), ctypes.byref(o)))
+
+    def close(self):
+        if self._ctx:
+            _lib().pac_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stream(self):
+        """The engine's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
+        return _lib().pac_cuda_stream(self._ctx) or 0
+
+    def alpha_complex(self, balls, sol_rad, alpha):
+        """balls: (n, 4) float32 (x, y, z, raw radius) on the host."""
+        b = np.ascontiguousarray(balls, dtype=np.float32)
+        if b.ndim != 2 or b.shape[1] != 4:
+            raise ValueError("balls must have shape (n, 4)")
+        cx, st = Complex(), Stats()
+        _check(_lib().pac_alpha_complex(self._ctx, b.ctypes.data_as(ctypes.c_void_p), len(b),
+                                        float(sol_rad), float(alpha), ctypes.byref(cx),
+                                        ctypes.byref(st)))
+        try:
+            return Result(_arr(cx.edges, cx.n_edges, 2), _arr(cx.tris, cx.n_tris, 3),
+                          _arr(cx.tets, cx.n_tets, 4), st.as_dict())
+        finally:
+            _lib().pac_free_complex(ctypes.byref(cx))
+
+    def alpha_complex_device(self, d_balls_ptr, n, sol_rad, alpha):
+        """Device-resident input (a device pointer, e.g. a torch tensor's
+        data_ptr()); returns (Complex with device pointers, stats).  The
+        lists stay valid until the next call on this engine."""
+        cx, st = Complex(), Stats()
+        _check(_lib().pac_alpha_complex_device(self._ctx, ctypes.c_void_p(d_balls_ptr), n,
+                                               float(sol_rad), float(alpha), ctypes.byref(cx),
+                                               ctypes.byref(st)))
+        return cx, st.as_dict()
+
+    def alpha_complex_batch(self, balls, offsets, sol_rad, alpha):
+        """Many molecules back to back; offsets has n_mol + 1 entries.
+        Returns a list of Result (molecule-local indices) and the stats."""
+        b = np.ascontiguousarray(balls, dtype=np.float32)
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        nm = len(off) - 1
+        bc, st = BatchComplex(), Stats()
+        _check(_lib().pac_alpha_complex_batch(self._ctx, b.ctypes.data_as(ctypes.c_void_p),
+                                              off.ctypes.data_as(ctypes.c_void_p), nm,
+                                              float(sol_rad), float(alpha), ctypes.byref(bc),
+                                              ctypes.byref(st)))
+        try:
+            eo = np.ctypeslib.as_array(bc.edge_off, (nm + 1,)).copy()
+            to = np.ctypeslib.as_array(bc.tri_off, (nm + 1,)).copy()
+            qo = np.ctypeslib.as_array(bc.tet_off, (nm + 1,)).copy()
+            E = _arr(bc.edges, int(eo[-1]), 2)
+            T = _arr(bc.tris, int(to[-1]), 3)
+            Q = _arr(bc.tets, int(qo[-1]), 4)
+            res = [Result(E[eo[m]:eo[m + 1]], T[to[m]:to[m + 1]], Q[qo[m]:qo[m + 1]], None)
+                   for m in range(nm)]
+            return res, st.as_dict()
+        finally:
+            _lib().pac_free_batch_complex(ctypes.byref(bc))
+
+
+def read_crd(path):
+    """(n, 4) float32 balls of a CRD file, parsed like the reference."""
+    L = _lib()
+    p = ctypes.c_void_p()
+    n = ctypes.c_uint32()
+    _check(L.pac_read_crd(os.fsencode(path), ctypes.byref(p), ctypes.byref(n)))
+    try:
+        if n.value == 0:
+            return np.zeros((0, 4), np.float32)
+        buf = (ctypes.c_float * (4 * n.value)).from_address(p.value)
+        return np.frombuffer(buf, dtype=np.float32).reshape(n.value, 4).copy()
+    finally:
+        ctypes.CDLL(None).free(p)
+
+
+def write_complex(path, balls, sol_rad, result):
+    """Write `result` in the reference's output file format."""
+    b = np.ascontiguousarray(balls, dtype=np.float32)
+    E = np.ascontiguousarray(result.edges, dtype=np.uint32)
+    T = np.ascontiguousarray(result.tris, dtype=np.uint32)
+    Q = np.ascontiguousarray(result.tets, dtype=np.uint32)
+    cx = Complex(len(b), 0, len(E), len(T), len(Q),
+                 E.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                 T.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                 Q.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    _check(_lib().pac_write_complex(os.fsencode(path), b.ctypes.data_as(ctypes.c_void_p), len(b),
+                                    float(sol_rad), ctypes.byref(cx)))
+
+
+# ----------------------------------------------------------------- workloads
+def _synth():
+    global _SYNTH
+    if _SYNTH is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise RuntimeError("libpac_synth.so is not built; run parallelac-xmp_b200/build.py")
+        S = ctypes.CDLL(SYNTH_PATH)
+        S.pac_synth_globule.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p]
+        S.pac_synth_snapped.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_void_p]
+        S.pac_synth_assembly.argtypes = [ctypes.c_uint64] + [ctypes.c_uint32] * 4 + [
+            ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+        S.pac_synth_batch_sizes.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_uint32, ctypes.c_void_p]
+        S.pac_synth_batch.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+        _SYNTH = S
+    return _SYNTH
+
+
+SEED_BASE = 0xA1FA0000
+
+
+def globule(n, seed=SEED_BASE):
+    """Self-avoiding-walk globule of n balls at 0.05 balls/A^3."""
+    out = np.zeros((n, 4), np.float32)
+    if _synth().pac_synth_globule(seed, n, out.ctypes.data) != 0:
+        raise MemoryError("generator allocation failed")
+    return out
+
+
+def snapped_globule(n, seed=SEED_BASE + 1, grid=0.25, rq=0.05):
+    """Globule with centres on a `grid` lattice and radii quantised to `rq`."""
+    out = np.zeros((n, 4), np.float32)
+    if _synth().pac_synth_snapped(seed, n, grid, rq, out.ctypes.data) != 0:
+        raise MemoryError("generator allocation failed")
+    return out
+
+
+def assembly(nx=8, ny=10, nz=5, per=6250, pitch=60.0, side=57.0, seed=SEED_BASE + 2):
+    """nx*ny*nz cube-confined globules on a lattice (the 2.5M-ball assembly)."""
+    out = np.zeros((nx * ny * nz * per, 4), np.float32)
+    if _synth().pac_synth_assembly(seed, nx, ny, nz, per, pitch, side, out.ctypes.data) != 0:
+        raise MemoryError("generator allocation failed")
+    return out
+
+
+def batch_sizes(count=4096, lo=200, hi=20000, seed=SEED_BASE + 3):
+    s = np.zeros(count, np.uint32)
+    _synth().pac_synth_batch_sizes(seed, count, lo, hi, s.ctypes.data)
+    return s
+
+
+def batch(sizes, seed=SEED_BASE + 3):
+    """Molecules of the given sizes back to back, and their offsets."""
+    sizes = np.ascontiguousarray(sizes, dtype=np.uint32)
+    off = np.zeros(len(sizes) + 1, np.uint64)
+    off[1:] = np.cumsum(sizes.astype(np.uint64))
+    out = np.zeros((int(off[-1]), 4), np.float32)
+    if _synth().pac_synth_batch(seed, len(sizes), sizes.ctypes.data, out.ctypes.data) != 0:
+        raise MemoryError("generator allocation failed")
+    return out, off

@@ -1,0 +1,548 @@
+// engine.cu -- the extern "C" API of libpac.so (declared in include/pac.h):
+// context and device memory pool, the host/device/batched entry points,
+// CRD input and the reference's text output format.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pac_internal.h"
+
+struct pac_ctx {
+    pac::Ctx c;
+};
+
+namespace pac {
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const std::string &msg) {
+    g_last_error = msg;
+    return status;
+}
+
+Arena::~Arena() {
+    for (auto &b : blocks_) cudaFree(b.base);
+}
+
+void *Arena::alloc(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    while (cur_ < blocks_.size()) {
+        Block &b = blocks_[cur_];
+        if (b.used + bytes <= b.size) {
+            void *p = b.base + b.used;
+            b.used += bytes;
+            return p;
+        }
+        cur_++;
+    }
+    size_t sz = std::max<size_t>(bytes, size_t(256) << 20);
+    char *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, sz);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(PAC_ERR_OOM, std::string("cudaMalloc(") + std::to_string(sz) +
+                                   "): " + cudaGetErrorString(e));
+        return nullptr;
+    }
+    blocks_.push_back(Block{p, sz, bytes});
+    cur_ = blocks_.size() - 1;
+    return p;
+}
+
+void Arena::reset() {
+    // merge: if more than one block was needed, replace them by one block
+    // large enough for the whole previous call, so later calls are served
+    // from a single region
+    if (blocks_.size() > 1) {
+        size_t total = 0;
+        for (auto &b : blocks_) total += b.size;
+        for (auto &b : blocks_) cudaFree(b.base);
+        blocks_.clear();
+        char *p = nullptr;
+        if (cudaMalloc(&p, total) == cudaSuccess)
+            blocks_.push_back(Block{p, total, 0});
+        else
+            cudaGetLastError();
+    }
+    for (auto &b : blocks_) b.used = 0;
+    cur_ = 0;
+}
+
+size_t Arena::reserved() const {
+    size_t t = 0;
+    for (auto &b : blocks_) t += b.size;
+    return t;
+}
+
+}  // namespace pac
+
+// ----------------------------------------------------------------- helpers
+namespace {
+
+__global__ void k_check_finite(const float4 *b, uint64_t n, int *bad) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = b[i];
+    if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
+}
+
+int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
+        const uint64_t *h_off, float sol, float alpha, pac::PassOutput &out, pac_stats *st) {
+    pac::Ctx &c = ctx->c;
+    if (!std::isfinite(sol) || !std::isfinite(alpha))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "sol_rad and alpha must be finite");
+    int *bad = c.arena.alloc_n<int>(1);
+    if (!bad) return PAC_ERR_OOM;
+    cudaMemsetAsync(bad, 0, sizeof(int), c.stream);
+    k_check_finite<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(d_balls, n, bad);
+    int hbad = 0;
+    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("input check: ") + cudaGetErrorString(e));
+    if (hbad) return pac::set_error(PAC_ERR_INVALID_ARG, "non-finite ball coordinate or radius");
+    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose};
+    pac::PassInput in{d_balls, n, n_mol, h_off, sol, alpha};
+    int rc = (c.opt.predicates == PAC_PRED_REFCOMPAT_FMA)
+                 ? pac_fma::run_pass(c, cfg, in, out, st)
+                 : pac_strict::run_pass(c, cfg, in, out, st);
+    if (rc == PAC_OK) {
+        e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess)
+            return pac::set_error(PAC_ERR_CUDA, std::string("pass: ") + cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+int validate_opts(const pac_options &o) {
+    if (o.formula != PAC_FORMULA_UPSTREAM && o.formula != PAC_FORMULA_PLAIN_XMP)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "unknown formula");
+    if (o.tet_mode != PAC_TETS_AS_WRITTEN && o.tet_mode != PAC_TETS_AS_RUN)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "unknown tet_mode");
+    if (o.predicates != PAC_PRED_REFCOMPAT && o.predicates != PAC_PRED_REFCOMPAT_FMA)
+        return pac::set_error(PAC_ERR_INVALID_ARG,
+                              o.predicates == PAC_PRED_EXACT
+                                  ? "PAC_PRED_EXACT is not available in this build"
+                                  : "unknown predicate mode");
+    if (o.order != PAC_ORDER_REFERENCE && o.order != PAC_ORDER_CANONICAL)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "unknown order");
+    return PAC_OK;
+}
+
+template <class T>
+int to_pinned(const T *d, uint64_t count, T **h, cudaStream_t s) {
+    *h = nullptr;
+    if (!count) return PAC_OK;
+    if (cudaMallocHost((void **)h, sizeof(T) * count) != cudaSuccess) {
+        cudaGetLastError();
+        return pac::set_error(PAC_ERR_OOM, "cudaMallocHost for the output lists failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(*h, d, sizeof(T) * count, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    return PAC_OK;
+}
+
+// in-place canonical order on the host copy: ascending vertices within each
+// simplex, rows sorted lexicographically
+template <int K>
+void canonicalise(uint32_t *rows, uint64_t nrows) {
+    struct Row {
+        uint32_t v[K];
+        bool operator<(const Row &o) const {
+            for (int i = 0; i < K; i++)
+                if (v[i] != o.v[i]) return v[i] < o.v[i];
+            return false;
+        }
+    };
+    Row *r = reinterpret_cast<Row *>(rows);
+    for (uint64_t i = 0; i < nrows; i++) {
+        for (int a = 1; a < K; a++)
+            for (int b = a; b > 0 && r[i].v[b] < r[i].v[b - 1]; b--) {
+                uint32_t t = r[i].v[b];
+                r[i].v[b] = r[i].v[b - 1];
+                r[i].v[b - 1] = t;
+            }
+    }
+    std::sort(r, r + nrows);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- C ABI
+extern "C" {
+
+int pac_abi_version(void) { return PAC_ABI_VERSION; }
+
+void pac_default_options(pac_options *opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->device = 0;
+    opt->formula = PAC_FORMULA_UPSTREAM;
+    opt->tet_mode = PAC_TETS_AS_WRITTEN;
+    opt->predicates = PAC_PRED_REFCOMPAT;
+    opt->order = PAC_ORDER_REFERENCE;
+}
+
+int pac_create(pac_ctx **out, const pac_options *opt) {
+    if (!out) return pac::set_error(PAC_ERR_INVALID_ARG, "ctx is null");
+    *out = nullptr;
+    pac_options o;
+    pac_default_options(&o);
+    if (opt) o = *opt;
+    int rc = validate_opts(o);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return pac::set_error(PAC_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (o.device < 0 || o.device >= ndev)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "device ordinal out of range");
+    cudaError_t e = cudaSetDevice(o.device);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    pac_ctx *c = new pac_ctx();
+    c->c.device = o.device;
+    c->c.opt = o;
+    if (cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return pac::set_error(PAC_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    for (auto &ev : c->c.ev) cudaEventCreate(&ev);
+    *out = c;
+    return PAC_OK;
+}
+
+int pac_destroy(pac_ctx *ctx) {
+    if (!ctx) return PAC_OK;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    for (auto &ev : ctx->c.ev)
+        if (ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return PAC_OK;
+}
+
+void *pac_cuda_stream(pac_ctx *ctx) { return ctx ? (void *)ctx->c.stream : nullptr; }
+
+int pac_alpha_complex_device(pac_ctx *ctx, const pac_ball *d_balls, uint32_t n, float sol_rad,
+                             float alpha, pac_complex *out, pac_stats *st) {
+    if (!ctx || !out || (n && !d_balls))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->n_vertices = n;
+    out->on_device = 1;
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (n == 0) return PAC_OK;
+    pac::Ctx &c = ctx->c;
+    cudaSetDevice(c.device);
+    c.arena.reset();
+    c.launches = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    uint64_t off[2] = {0, n};
+    pac::PassOutput po;
+    int rc = run(ctx, reinterpret_cast<const float4 *>(d_balls), n, 1, off, sol_rad, alpha, po, st);
+    cudaEventRecord(e1, c.stream);
+    cudaEventSynchronize(e1);
+    if (st && !rc) {
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        st->ms_total = t;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    out->n_edges = po.n_edges;
+    out->n_tris = po.n_tris;
+    out->n_tets = po.n_tets;
+    out->edges = po.d_edges;
+    out->tris = po.d_tris;
+    out->tets = po.d_tets;
+    if (st) st->kernels_launched = (uint32_t)c.launches;
+    return PAC_OK;
+}
+
+int pac_alpha_complex(pac_ctx *ctx, const pac_ball *balls, uint32_t n, float sol_rad, float alpha,
+                      pac_complex *out, pac_stats *st) {
+    if (!ctx || !out || (n && !balls)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->n_vertices = n;
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (n == 0) return PAC_OK;
+    pac::Ctx &c = ctx->c;
+    cudaSetDevice(c.device);
+    c.arena.reset();
+    c.launches = 0;
+    cudaEvent_t e0, e1, e2, e3;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventCreate(&e3);
+    cudaEventRecord(e0, c.stream);
+    float4 *d = c.arena.alloc_n<float4>(n);
+    if (!d) return PAC_ERR_OOM;
+    cudaError_t e = cudaMemcpyAsync(d, balls, sizeof(float4) * n, cudaMemcpyHostToDevice, c.stream);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("H2D: ") + cudaGetErrorString(e));
+    cudaEventRecord(e1, c.stream);
+    uint64_t off[2] = {0, n};
+    pac::PassOutput po;
+    int rc = run(ctx, d, n, 1, off, sol_rad, alpha, po, st);
+    if (rc) return rc;
+    cudaEventRecord(e2, c.stream);
+    out->n_edges = po.n_edges;
+    out->n_tris = po.n_tris;
+    out->n_tets = po.n_tets;
+    out->on_device = 2;  // pinned host memory
+    if ((rc = to_pinned(po.d_edges, 2 * po.n_edges, &out->edges, c.stream)) ||
+        (rc = to_pinned(po.d_tris, 3 * po.n_tris, &out->tris, c.stream)) ||
+        (rc = to_pinned(po.d_tets, 4 * po.n_tets, &out->tets, c.stream))) {
+        pac_free_complex(out);
+        return rc;
+    }
+    cudaEventRecord(e3, c.stream);
+    e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess) {
+        pac_free_complex(out);
+        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    }
+    if (c.opt.order == PAC_ORDER_CANONICAL) {
+        canonicalise<2>(out->edges, out->n_edges);
+        canonicalise<3>(out->tris, out->n_tris);
+        canonicalise<4>(out->tets, out->n_tets);
+    }
+    if (st) {
+        float a = 0, b = 0, t = 0;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, e2, e3);
+        cudaEventElapsedTime(&t, e0, e3);
+        st->ms_h2d = a;
+        st->ms_d2h = b;
+        st->ms_total = t;
+        st->kernels_launched = (uint32_t)c.launches;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    cudaEventDestroy(e3);
+    return PAC_OK;
+}
+
+int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t *offsets,
+                            uint32_t n_mol, float sol_rad, float alpha, pac_batch_complex *out,
+                            pac_stats *st) {
+    if (!ctx || !out || !offsets || n_mol == 0)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "null argument or no molecules");
+    std::memset(out, 0, sizeof(*out));
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (offsets[0] != 0) return pac::set_error(PAC_ERR_INVALID_ARG, "offsets[0] must be 0");
+    for (uint32_t m = 0; m < n_mol; m++)
+        if (offsets[m + 1] < offsets[m])
+            return pac::set_error(PAC_ERR_INVALID_ARG, "offsets must be non-decreasing");
+    uint64_t n = offsets[n_mol];
+    if (n >= 0xffffffffull) return pac::set_error(PAC_ERR_CAPACITY, "more than 2^32-1 balls");
+    if (n && !balls) return pac::set_error(PAC_ERR_INVALID_ARG, "balls is null");
+    // empty molecules are carried as zero-length ranges; the pass itself
+    // needs at least one ball per molecule, so drop them and re-expand
+    std::vector<uint32_t> keep;
+    std::vector<uint64_t> koff(1, 0);
+    for (uint32_t m = 0; m < n_mol; m++)
+        if (offsets[m + 1] > offsets[m]) {
+            keep.push_back(m);
+            koff.push_back(offsets[m + 1]);
+        }
+    out->n_mol = n_mol;
+    out->on_device = 2;
+    out->edge_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
+    out->tri_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
+    out->tet_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
+    if (!out->edge_off || !out->tri_off || !out->tet_off) {
+        pac_free_batch_complex(out);
+        return pac::set_error(PAC_ERR_OOM, "host allocation failed");
+    }
+    if (keep.empty()) return PAC_OK;
+    pac::Ctx &c = ctx->c;
+    cudaSetDevice(c.device);
+    c.arena.reset();
+    c.launches = 0;
+    cudaEvent_t e0, e3;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e3);
+    cudaEventRecord(e0, c.stream);
+    float4 *d = c.arena.alloc_n<float4>(n);
+    if (!d) return PAC_ERR_OOM;
+    cudaMemcpyAsync(d, balls, sizeof(float4) * n, cudaMemcpyHostToDevice, c.stream);
+    pac::PassOutput po;
+    int rc = run(ctx, d, n, (uint32_t)keep.size(), koff.data(), sol_rad, alpha, po, st);
+    if (rc) {
+        pac_free_batch_complex(out);
+        return rc;
+    }
+    if ((rc = to_pinned(po.d_edges, 2 * po.n_edges, &out->edges, c.stream)) ||
+        (rc = to_pinned(po.d_tris, 3 * po.n_tris, &out->tris, c.stream)) ||
+        (rc = to_pinned(po.d_tets, 4 * po.n_tets, &out->tets, c.stream))) {
+        pac_free_batch_complex(out);
+        return rc;
+    }
+    cudaEventRecord(e3, c.stream);
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess) {
+        pac_free_batch_complex(out);
+        return pac::set_error(PAC_ERR_CUDA, std::string("batch: ") + cudaGetErrorString(e));
+    }
+    // re-expand the row offsets over all molecules
+    size_t k = 0;
+    for (uint32_t m = 0; m <= n_mol; m++) {
+        while (k < keep.size() && keep[k] < m) k++;
+        out->edge_off[m] = po.edge_off[k];
+        out->tri_off[m] = po.tri_off[k];
+        out->tet_off[m] = po.tet_off[k];
+    }
+    if (c.opt.order == PAC_ORDER_CANONICAL)
+        for (uint32_t m = 0; m < n_mol; m++) {
+            canonicalise<2>(out->edges + 2 * out->edge_off[m], out->edge_off[m + 1] - out->edge_off[m]);
+            canonicalise<3>(out->tris + 3 * out->tri_off[m], out->tri_off[m + 1] - out->tri_off[m]);
+            canonicalise<4>(out->tets + 4 * out->tet_off[m], out->tet_off[m + 1] - out->tet_off[m]);
+        }
+    if (st) {
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e3);
+        st->ms_total = t;
+        st->kernels_launched = (uint32_t)c.launches;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e3);
+    return PAC_OK;
+}
+
+void pac_free_complex(pac_complex *cx) {
+    if (!cx) return;
+    if (cx->on_device == 2) {
+        if (cx->edges) cudaFreeHost(cx->edges);
+        if (cx->tris) cudaFreeHost(cx->tris);
+        if (cx->tets) cudaFreeHost(cx->tets);
+    } else if (cx->on_device == 0) {
+        std::free(cx->edges);
+        std::free(cx->tris);
+        std::free(cx->tets);
+    }
+    // on_device == 1: lists live in the context's pool until its next call
+    cx->edges = cx->tris = cx->tets = nullptr;
+    cx->n_edges = cx->n_tris = cx->n_tets = 0;
+}
+
+void pac_free_batch_complex(pac_batch_complex *cx) {
+    if (!cx) return;
+    if (cx->on_device == 2) {
+        if (cx->edges) cudaFreeHost(cx->edges);
+        if (cx->tris) cudaFreeHost(cx->tris);
+        if (cx->tets) cudaFreeHost(cx->tets);
+    }
+    std::free(cx->edge_off);
+    std::free(cx->tri_off);
+    std::free(cx->tet_off);
+    std::memset(cx, 0, sizeof(*cx));
+}
+
+const char *pac_status_string(int status) {
+    switch (status) {
+        case PAC_OK: return "ok";
+        case PAC_ERR_INVALID_ARG: return "invalid argument";
+        case PAC_ERR_CUDA: return "CUDA error";
+        case PAC_ERR_CAPACITY: return "capacity exceeded";
+        case PAC_ERR_TIMEOUT: return "device wait timed out";
+        case PAC_ERR_NO_DEVICE: return "no CUDA device";
+        case PAC_ERR_EXACT_RANGE: return "exact arithmetic range exceeded";
+        case PAC_ERR_OOM: return "out of memory";
+        case PAC_ERR_IO: return "I/O error";
+        default: return "unknown status";
+    }
+}
+
+const char *pac_last_error(void) { return pac::g_last_error.c_str(); }
+
+// CRD input: the reference reads the count with "%d" and each ball with
+// "%f %f %f %f" (AlphaComplexLargeData.cu:1070, 1079); strtof gives the same
+// correctly rounded floats.
+int pac_read_crd(const char *path, pac_ball **balls, uint32_t *n) {
+    if (!path || !balls || !n) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    *balls = nullptr;
+    *n = 0;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return pac::set_error(PAC_ERR_IO, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    long sz = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    std::vector<char> buf((size_t)std::max(sz, 0L) + 1);
+    size_t got = std::fread(buf.data(), 1, (size_t)std::max(sz, 0L), f);
+    std::fclose(f);
+    buf[got] = 0;
+    char *p = buf.data(), *end = nullptr;
+    errno = 0;
+    long cnt = std::strtol(p, &end, 10);
+    if (end == p || cnt < 0 || cnt > 0xfffffffeL)
+        return pac::set_error(PAC_ERR_IO, std::string("bad ball count in ") + path);
+    p = end;
+    pac_ball *b = (pac_ball *)std::malloc(sizeof(pac_ball) * (size_t)(cnt ? cnt : 1));
+    if (!b) return pac::set_error(PAC_ERR_OOM, "host allocation failed");
+    for (long i = 0; i < cnt; i++) {
+        float v[4];
+        for (int k = 0; k < 4; k++) {
+            v[k] = std::strtof(p, &end);
+            if (end == p) {
+                std::free(b);
+                return pac::set_error(PAC_ERR_IO, std::string(path) + ": ball " +
+                                                      std::to_string(i) + " is truncated");
+            }
+            p = end;
+        }
+        b[i] = pac_ball{v[0], v[1], v[2], v[3]};
+    }
+    *balls = b;
+    *n = (uint32_t)cnt;
+    return PAC_OK;
+}
+
+// The reference's output file (AlphaComplexLargeData.cu:2028-2050).
+int pac_write_complex(const char *path, const pac_ball *balls, uint32_t n, float sol_rad,
+                      const pac_complex *cx) {
+    if (!path || !cx || (n && !balls)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    if (cx->on_device == 1)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "complex lists are in device memory");
+    FILE *fp = std::fopen(path, "w");
+    if (!fp) return pac::set_error(PAC_ERR_IO, std::string("cannot create ") + path);
+    std::vector<char> obuf(1 << 20);
+    std::setvbuf(fp, obuf.data(), _IOFBF, obuf.size());
+    std::fprintf(fp, "%d %ld %ld %ld\n", (int)n, (long)cx->n_edges, (long)cx->n_tris,
+                 (long)cx->n_tets);
+    for (uint32_t i = 0; i < n; i++) {
+        float r = balls[i].r + sol_rad;
+        std::fprintf(fp, "%9.5lf %9.5lf %9.5lf %9.5lf\n", (double)balls[i].x, (double)balls[i].y,
+                     (double)balls[i].z, (double)r);
+    }
+    for (uint64_t i = 0; i < cx->n_edges; i++)
+        std::fprintf(fp, "%9d %9d\n", (int)cx->edges[2 * i], (int)cx->edges[2 * i + 1]);
+    for (uint64_t i = 0; i < cx->n_tris; i++)
+        std::fprintf(fp, "%9d %9d %9d\n", (int)cx->tris[3 * i], (int)cx->tris[3 * i + 1],
+                     (int)cx->tris[3 * i + 2]);
+    for (uint64_t i = 0; i < cx->n_tets; i++)
+        std::fprintf(fp, "%9d %9d %9d %9d\n", (int)cx->tets[4 * i], (int)cx->tets[4 * i + 1],
+                     (int)cx->tets[4 * i + 2], (int)cx->tets[4 * i + 3]);
+    int bad = std::ferror(fp);
+    if (std::fclose(fp) != 0 || bad) return pac::set_error(PAC_ERR_IO, std::string("write failed: ") + path);
+    return PAC_OK;
+}
+
+}  // extern "C"

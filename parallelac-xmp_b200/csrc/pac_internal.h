@@ -1,0 +1,83 @@
+// pac_internal.h -- types shared by the C ABI layer (engine.cu) and the
+// pipeline translation unit (pipeline.cu, compiled once per arithmetic
+// flavour).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pac.h"
+
+namespace pac {
+
+// Device memory pool: a list of large blocks handed out by bumping an
+// offset; reset() makes everything reusable without freeing, so repeated
+// calls on a context allocate nothing after the first.
+class Arena {
+   public:
+    ~Arena();
+    // 256-byte aligned; returns nullptr and records the error on failure
+    void *alloc(size_t bytes);
+    template <class T>
+    T *alloc_n(size_t n) {
+        return static_cast<T *>(alloc(sizeof(T) * (n ? n : 1)));
+    }
+    void reset();
+    size_t reserved() const;
+
+   private:
+    struct Block {
+        char *base;
+        size_t size, used;
+    };
+    std::vector<Block> blocks_;
+    size_t cur_ = 0;
+};
+
+struct PipelineConfig {
+    int formula;    // pac_formula
+    int tet_mode;   // pac_tet_mode
+    int verbose;
+};
+
+// Inputs of one device pass over one or more molecules.
+struct PassInput {
+    const float4 *d_balls;      // n x (x, y, z, raw r), molecules back to back
+    uint64_t n;                 // total balls
+    uint32_t n_mol;             // molecules
+    const uint64_t *h_offsets;  // n_mol + 1 (host)
+    float sol, alpha;
+};
+
+// Device-resident result of a pass: lists in reference order with
+// molecule-local 0-based input indices, and per-molecule row offsets.
+struct PassOutput {
+    uint32_t *d_edges = nullptr, *d_tris = nullptr, *d_tets = nullptr;
+    uint64_t n_edges = 0, n_tris = 0, n_tets = 0;
+    std::vector<uint64_t> edge_off, tri_off, tet_off;  // n_mol + 1 (host)
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    pac_options opt{};
+    cudaEvent_t ev[16]{};
+    int launches = 0;
+};
+
+// Sets the thread-local error detail; returns status.
+int set_error(int status, const std::string &msg);
+
+}  // namespace pac
+
+namespace pac_strict {
+int run_pass(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
+             pac::PassOutput &out, pac_stats *st);
+}
+namespace pac_fma {
+int run_pass(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
+             pac::PassOutput &out, pac_stats *st);
+}

@@ -1,0 +1,1452 @@
+// pipeline.cu -- the single device pass: balls in, weighted alpha complex out.
+//
+// Compiled twice: with -DPAC_NS=pac_strict -fmad=false (IEEE op-by-op, the
+// oracle-identical flavour) and with -DPAC_NS=pac_fma -fmad=true (nvcc's
+// default contraction, the flavour that follows the reference binary built
+// with default flags).  Nothing else differs between the two.
+//
+// Layout in HBM (n balls, molecules back to back):
+//   at[n]        float4 (x, y, z, r + sol) in (molecule, cell, input index)
+//                order -- the reference's stable sort by cell key
+//                (AlphaComplexLargeData.cu:1174-1177)
+//   orig[n]      molecule-local 0-based input index of each sorted ball
+//   cellbeg[]    CSR cell ranges over the sorted balls (all molecules)
+//   eoff[n+1], ER[]   alpha edges (i, ER[k]) with i < ER[k], CSR by i,
+//                each row ascending (= the reference's sorted edge list)
+//   loff[n+1], link[] per ball i, a deg(i) x deg(i) bit matrix over the
+//                row of i in ER: bit (a, b) set <=> (i, ER[a], ER[b]) is an
+//                alpha triangle.  faces[] has the same shape and marks final
+//                triangles.
+// Candidate tetrahedra are never stored: one kernel enumerates them from
+// the link matrices, applies the alpha filter and the empty-orthosphere
+// test, and writes only the survivors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pac_internal.h"
+#include "refarith.cuh"
+#include "sos.cuh"
+
+#ifndef PAC_NS
+#error "PAC_NS must name the arithmetic flavour namespace"
+#endif
+
+namespace PAC_NS {
+
+using pac::Ball;
+
+constexpr int kMaxDeg = 256;  // upper neighbours per ball supported
+constexpr int kMaxW = kMaxDeg / 64;
+constexpr unsigned kFull = 0xffffffffu;
+
+// device-side counters (one slot each)
+enum Counter {
+    C_CAND_E, C_ALPHA_E, C_CAND_T, C_ALPHA_T, C_CAND_Q, C_ALPHA_Q, C_INSPHERE, C_SOS,
+    C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NCOUNTERS
+};
+
+struct MolGrid {
+    float minx, miny, minz, step;
+    int gx, gy, gz, pad;
+    uint64_t cell_base;  // first global cell of this molecule
+    uint64_t ncell;
+    uint64_t atom_base;  // first ball (sorted and input) of this molecule
+};
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return pac::set_error(PAC_ERR_CUDA, std::string(#call) + ": " +               \
+                                                    cudaGetErrorString(e_));              \
+    } while (0)
+
+#define LAUNCH_CHECK(ctx)                                                                 \
+    do {                                                                                  \
+        (ctx).launches++;                                                                 \
+        cudaError_t e_ = cudaGetLastError();                                              \
+        if (e_ != cudaSuccess)                                                            \
+            return pac::set_error(PAC_ERR_CUDA, std::string("launch: ") +                 \
+                                                    cudaGetErrorString(e_));              \
+    } while (0)
+
+// ------------------------------------------------------------------ utils
+__device__ __forceinline__ int fkey(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float funkey(int k) {
+    return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff);
+}
+__device__ __forceinline__ uint32_t mol_of(const uint32_t *mol, uint64_t i) {
+    return mol ? mol[i] : 0u;
+}
+// 32-bit wrapping linear cell index, as the reference's int arithmetic
+// behaves on the GPU (AlphaComplexLargeData.cu:625-626).
+__device__ __forceinline__ int lin3(int X, int Y, int Z, int gx, int gy) {
+    return (int)((unsigned)Z * (unsigned)gx * (unsigned)gy + (unsigned)Y * (unsigned)gx +
+                 (unsigned)X);
+}
+// lower_bound of v in sorted a[0..n)
+__device__ __forceinline__ int lbound(const uint32_t *a, int n, uint32_t v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int m = (lo + hi) >> 1;
+        if (__ldg(&a[m]) < v)
+            lo = m + 1;
+        else
+            hi = m;
+    }
+    return lo;
+}
+// position of the k-th set bit (0-based) of a W-word mask, or -1
+__device__ __forceinline__ int select_bit(const uint64_t *m, int W, int k) {
+    for (int w = 0; w < W; w++) {
+        int c = __popcll(m[w]);
+        if (k < c) {
+            uint32_t lo = (uint32_t)m[w], hi = (uint32_t)(m[w] >> 32);
+            int cl = __popc(lo);
+            if (k < cl) return w * 64 + __fns(lo, 0, k + 1);
+            return w * 64 + 32 + __fns(hi, 0, k - cl + 1);
+        }
+        k -= c;
+    }
+    return -1;
+}
+// bits of word w whose global position is greater than b
+__device__ __forceinline__ uint64_t above_mask(int b, int w) {
+    if (w * 64 + 63 <= b) return 0ull;
+    if (w * 64 > b) return ~0ull;
+    int j = b & 63;
+    return j == 63 ? 0ull : (~0ull << (j + 1));
+}
+__device__ __forceinline__ void bump(unsigned long long *ctr, int which, unsigned long long v) {
+    if (v) atomicAdd(&ctr[which], v);
+}
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ scan
+// Exclusive prefix sum of n values into out[0..n], out[n] = total.
+template <class Tin>
+__global__ void k_scan_reduce(const Tin *in, uint64_t n, uint64_t *bsum) {
+    __shared__ uint64_t s[32];
+    uint64_t base = (uint64_t)blockIdx.x * 4096;
+    uint64_t acc = 0;
+    for (int k = 0; k < 4; k++) {
+        uint64_t i = base + (uint64_t)k * 1024 + threadIdx.x;
+        if (i < n) acc += (uint64_t)in[i];
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint64_t v = s[threadIdx.x];
+        v = warp_sum(v);
+        if (threadIdx.x == 0) bsum[blockIdx.x] = v;
+    }
+}
+__global__ void k_scan_blocks(uint64_t *bsum, uint64_t nb) {
+    // single block: exclusive scan of nb block sums in place
+    __shared__ uint64_t s[1024];
+    uint64_t carry = 0;
+    for (uint64_t base = 0; base < nb; base += 1024) {
+        uint64_t i = base + threadIdx.x;
+        uint64_t v = i < nb ? bsum[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            uint64_t t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < nb) bsum[i] = carry + s[threadIdx.x] - v;
+        uint64_t tot = s[1023];
+        __syncthreads();
+        carry += tot;
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;
+}
+template <class Tin, class Tout>
+__global__ void k_scan_apply(const Tin *in, uint64_t n, const uint64_t *bsum, Tout *out) {
+    __shared__ uint64_t s[1024];
+    uint64_t base = (uint64_t)blockIdx.x * 4096;
+    uint64_t carry = bsum[blockIdx.x];
+    for (int k = 0; k < 4; k++) {
+        uint64_t i = base + (uint64_t)k * 1024 + threadIdx.x;
+        uint64_t v = i < n ? (uint64_t)in[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            uint64_t t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < n) out[i] = (Tout)(carry + s[threadIdx.x] - v);
+        uint64_t tot = s[1023];
+        __syncthreads();
+        carry += tot;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (Tout)bsum[gridDim.x];
+}
+
+template <class Tin, class Tout>
+static int exclusive_scan(pac::Ctx &ctx, const Tin *in, uint64_t n, Tout *out) {
+    uint64_t nb = (n + 4095) / 4096;
+    if (nb == 0) nb = 1;
+    uint64_t *bsum = ctx.arena.alloc_n<uint64_t>(nb + 1);
+    if (!bsum) return PAC_ERR_OOM;
+    k_scan_reduce<Tin><<<(unsigned)nb, 1024, 0, ctx.stream>>>(in, n, bsum);
+    LAUNCH_CHECK(ctx);
+    k_scan_blocks<<<1, 1024, 0, ctx.stream>>>(bsum, nb);
+    LAUNCH_CHECK(ctx);
+    k_scan_apply<Tin, Tout><<<(unsigned)nb, 1024, 0, ctx.stream>>>(in, n, bsum, out);
+    LAUNCH_CHECK(ctx);
+    return PAC_OK;
+}
+
+// ------------------------------------------------------------------ grid
+__global__ void k_mol_ids(const uint64_t *off, uint32_t n_mol, uint32_t *mol) {
+    uint32_t m = blockIdx.x;
+    if (m >= n_mol) return;
+    for (uint64_t i = off[m] + threadIdx.x; i < off[m + 1]; i += blockDim.x) mol[i] = m;
+}
+
+// min/max of raw x, y, z, r per molecule (AlphaComplexLargeData.cu:1088-1110).
+// Floats are compared through an order-preserving int key.
+__global__ void k_bbox(const float4 *balls, uint64_t n, const uint32_t *mol, int *mm) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool act = i < n;
+    uint32_t m = act ? mol_of(mol, i) : 0xffffffffu;
+    float4 b = act ? balls[i] : make_float4(0, 0, 0, 0);
+    int k[4] = {fkey(b.x), fkey(b.y), fkey(b.z), fkey(b.w)};
+    uint32_t m0 = __shfl_sync(kFull, m, 0);
+    bool uniform = __all_sync(kFull, act && m == m0);
+    for (int q = 0; q < 4; q++) {
+        if (uniform) {
+            int lo = k[q], hi = k[q];
+            for (int o = 16; o; o >>= 1) {
+                lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+                hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+            }
+            if ((threadIdx.x & 31) == 0) {
+                atomicMin(&mm[m * 8 + q], lo);
+                atomicMax(&mm[m * 8 + 4 + q], hi);
+            }
+        } else if (act) {
+            atomicMin(&mm[m * 8 + q], k[q]);
+            atomicMax(&mm[m * 8 + 4 + q], k[q]);
+        }
+    }
+}
+
+// grid parameters per molecule (AlphaComplexLargeData.cu:1119-1123)
+__global__ void k_grid(const int *mm, uint32_t n_mol, float alpha, MolGrid *g, uint64_t *ncell) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n_mol) return;
+    float minX = funkey(mm[m * 8 + 0]), minY = funkey(mm[m * 8 + 1]),
+          minZ = funkey(mm[m * 8 + 2]);
+    float maxX = funkey(mm[m * 8 + 4]), maxY = funkey(mm[m * 8 + 5]),
+          maxZ = funkey(mm[m * 8 + 6]), maxRadius = funkey(mm[m * 8 + 7]);
+    float possibleMaxRadius = __fsqrt_rn(__fadd_rn(__fmul_rn(maxRadius, maxRadius), alpha));
+    float stepSize = __fmul_rn(2.0f, possibleMaxRadius);
+    int gx = (int)__fdiv_rn(__fsub_rn(maxX, minX), stepSize) + 1;
+    int gy = (int)__fdiv_rn(__fsub_rn(maxY, minY), stepSize) + 1;
+    int gz = (int)__fdiv_rn(__fsub_rn(maxZ, minZ), stepSize) + 1;
+    MolGrid r;
+    r.minx = minX;
+    r.miny = minY;
+    r.minz = minZ;
+    r.step = stepSize;
+    r.gx = gx;
+    r.gy = gy;
+    r.gz = gz;
+    r.pad = 0;
+    r.cell_base = 0;
+    r.ncell = (uint64_t)max(gx, 0) * (uint64_t)max(gy, 0) * (uint64_t)max(gz, 0);
+    r.atom_base = 0;
+    g[m] = r;
+    ncell[m] = r.ncell;
+}
+
+// cell key (AlphaComplexLargeData.cu:65-78) and a slot within the cell
+__global__ void k_cellkey(const float4 *balls, uint64_t n, const uint32_t *mol, const MolGrid *g,
+                          uint32_t *gcell, uint32_t *slot, uint32_t *cellcnt) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const MolGrid G = g[mol_of(mol, i)];
+    float4 b = balls[i];
+    int cellX = (int)__fdiv_rn(__fsub_rn(b.x, G.minx), G.step);
+    int cellY = (int)__fdiv_rn(__fsub_rn(b.y, G.miny), G.step);
+    int cellZ = (int)__fdiv_rn(__fsub_rn(b.z, G.minz), G.step);
+    int cell = cellX + G.gx * cellY + G.gx * G.gy * cellZ;
+    uint32_t gc = (uint32_t)(G.cell_base + (uint64_t)cell);
+    gcell[i] = gc;
+    slot[i] = atomicAdd(&cellcnt[gc], 1u);
+}
+
+__global__ void k_scatter(uint64_t n, const uint32_t *gcell, const uint32_t *slot,
+                          const uint32_t *cellbeg, uint32_t *perm) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    perm[cellbeg[gcell[i]] + slot[i]] = (uint32_t)i;
+}
+
+// order each cell by input index: the stable sort's tie order
+__global__ void k_cellsort(uint64_t ncell, const uint32_t *cellbeg, uint32_t *perm) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    uint32_t b = cellbeg[c], e = cellbeg[c + 1];
+    for (uint32_t i = b + 1; i < e; i++) {
+        uint32_t v = perm[i];
+        uint32_t j = i;
+        while (j > b && perm[j - 1] > v) {
+            perm[j] = perm[j - 1];
+            j--;
+        }
+        perm[j] = v;
+    }
+}
+
+__global__ void k_gather(uint64_t n, const uint32_t *perm, const float4 *balls, float sol,
+                         const uint32_t *gcell, const uint32_t *mol, const MolGrid *g,
+                         float4 *at, uint32_t *orig, uint32_t *cellof) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint32_t i = perm[p];
+    float4 b = balls[i];
+    at[p] = make_float4(b.x, b.y, b.z, __fadd_rn(b.w, sol));
+    orig[p] = (uint32_t)(i - g[mol_of(mol, i)].atom_base);
+    cellof[p] = gcell[i];
+}
+
+// ------------------------------------------------------------------ edges
+// One warp per ball i: the candidates are the balls l > i of the 27 cells
+// around i's cell whose linear index is >= i's (AlphaComplexLargeData.cu:
+// 80-165); each passes the power filter (markRealEdges) or not.  Lane k < 27
+// owns neighbour cell k in the reference's loop order, so a warp prefix sum
+// over the cell sizes enumerates the candidates in ascending l.
+template <int V, bool FILL>
+__global__ void __launch_bounds__(256) k_edges(uint64_t n, const float4 *__restrict__ at,
+                                               const uint32_t *__restrict__ cellof,
+                                               const uint32_t *__restrict__ cellbeg,
+                                               const uint32_t *__restrict__ mol,
+                                               const MolGrid *__restrict__ grids, float alpha,
+                                               uint32_t *ecount, const uint64_t *eoff,
+                                               uint32_t *ER, unsigned long long *ctr) {
+    const int lane = threadIdx.x & 31;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long cand_acc = 0, alpha_acc = 0;
+    for (uint64_t p = warp; p < n; p += nwarps) {
+        const MolGrid G = grids[mol_of(mol, p)];
+        int cell = (int)(cellof[p] - G.cell_base);
+        int gX = cell % G.gx, t = cell / G.gx, gY = t % G.gy, gZ = t / G.gy;
+        uint32_t beg = 0, cnt = 0;
+        if (lane < 27) {
+            int i = lane / 9 - 1, j = (lane / 3) % 3 - 1, k = lane % 3 - 1;
+            bool ok = !((gZ + i >= G.gz) || (gY + j >= G.gy) || (gX + k >= G.gx)) &&
+                      !((gZ + i < 0) || (gY + j < 0) || (gX + k < 0));
+            if (ok) {
+                int adj = (gZ + i) * G.gx * G.gy + (gY + j) * G.gx + (gX + k);
+                if (adj >= cell) {
+                    uint64_t gc = G.cell_base + (uint64_t)adj;
+                    uint32_t b = cellbeg[gc], e = cellbeg[gc + 1];
+                    if (adj == cell) b = (uint32_t)p + 1;
+                    if (e > b) {
+                        beg = b;
+                        cnt = e - b;
+                    }
+                }
+            }
+        }
+        uint32_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        uint32_t total = __shfl_sync(kFull, incl, 31);
+        const Ball A = pac::ld_ball(&at[p]);
+        uint64_t out = FILL ? eoff[p] : 0;
+        uint32_t kept = 0;
+        for (uint32_t base = 0; base < total; base += 32) {
+            uint32_t s = base + lane;
+            bool act = s < total;
+            // segment owning slot s: first lane whose inclusive sum exceeds s
+            int lo = 0;
+            for (int step = 16; step; step >>= 1) {
+                uint32_t v = __shfl_sync(kFull, incl, lo + step - 1);
+                if (v <= s) lo += step;
+            }
+            uint32_t sinc = __shfl_sync(kFull, incl, lo & 31);
+            uint32_t sbeg = __shfl_sync(kFull, beg, lo & 31);
+            uint32_t scnt = __shfl_sync(kFull, cnt, lo & 31);
+            bool pass = false;
+            uint32_t l = 0;
+            if (act) {
+                l = sbeg + (s - (sinc - scnt));
+                pass = pac::edge_alpha<V>(A, pac::ld_ball(&at[l]), alpha);
+            }
+            unsigned m = __ballot_sync(kFull, pass);
+            if (FILL && pass) ER[out + kept + __popc(m & ((1u << lane) - 1))] = l;
+            kept += __popc(m);
+        }
+        if (lane == 0) {
+            if (!FILL) ecount[p] = kept;
+            cand_acc += total;
+            alpha_acc += kept;
+        }
+    }
+    if (!FILL && lane == 0) {
+        bump(ctr, C_CAND_E, cand_acc);
+        bump(ctr, C_ALPHA_E, alpha_acc);
+    }
+}
+
+// words of link matrix per ball
+__global__ void k_link_size(uint64_t n, const uint64_t *eoff, uint64_t *lsize,
+                            unsigned long long *ctr) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint64_t deg = eoff[p + 1] - eoff[p];
+    uint64_t W = (deg + 63) >> 6;
+    lsize[p] = deg * W;
+    atomicMax(&ctr[C_MAXDEG], (unsigned long long)deg);
+}
+
+// ------------------------------------------------------------------ triangles
+// One warp per ball i: bit (a, b) of i's link matrix is set when
+// (i, v1 = N[a], v2 = N[b]) is a candidate triangle -- edge v1v2 is an alpha
+// edge (AlphaComplexLargeData.cu:192-296) -- and passes markRealTriangles.
+template <int V>
+__global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restrict__ at,
+                                              const uint64_t *__restrict__ eoff,
+                                              const uint32_t *__restrict__ ER,
+                                              const uint64_t *__restrict__ loff, uint64_t *link,
+                                              float alpha, unsigned long long *ctr) {
+    __shared__ uint64_t srow[8][kMaxW];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long cand_acc = 0, alpha_acc = 0;
+    for (uint64_t p = warp; p < n; p += nwarps) {
+        const uint64_t e0 = eoff[p];
+        const int deg = (int)(eoff[p + 1] - e0);
+        if (deg < 2) continue;
+        const int W = (deg + 63) >> 6;
+        const uint32_t *N = ER + e0;
+        uint64_t *L = link + loff[p];
+        const Ball A = pac::ld_ball(&at[p]);
+        for (int a = 0; a < deg - 1; a++) {
+            if (lane < kMaxW) srow[wib][lane] = 0;
+            __syncwarp();
+            const uint32_t v1 = __ldg(&N[a]);
+            const Ball A1 = pac::ld_ball(&at[v1]);
+            const uint32_t *N1 = ER + eoff[v1];
+            const int deg1 = (int)(eoff[v1 + 1] - eoff[v1]);
+            for (int base = a + 1; base < deg; base += 32) {
+                int b = base + lane;
+                bool cand = false, pass = false;
+                if (b < deg) {
+                    uint32_t v2 = __ldg(&N[b]);
+                    int pos = lbound(N1, deg1, v2);
+                    cand = pos < deg1 && __ldg(&N1[pos]) == v2;
+                    if (cand) {
+                        float4 o;
+                        pass = pac::tri_alpha<V>(A, A1, pac::ld_ball(&at[v2]), alpha, o);
+                    }
+                }
+                unsigned cm = __ballot_sync(kFull, cand), pm = __ballot_sync(kFull, pass);
+                if (lane == 0) {
+                    cand_acc += __popc(cm);
+                    alpha_acc += __popc(pm);
+                    int w = base >> 6, sh = base & 63;
+                    srow[wib][w] |= (uint64_t)pm << sh;
+                    if (sh > 32 && w + 1 < kMaxW) srow[wib][w + 1] |= (uint64_t)pm >> (64 - sh);
+                }
+                __syncwarp();
+            }
+            if (lane < W) L[(uint64_t)a * W + lane] = srow[wib][lane];
+            __syncwarp();
+        }
+        if (lane < W) L[(uint64_t)(deg - 1) * W + lane] = 0;
+    }
+    if (lane == 0) {
+        bump(ctr, C_CAND_T, cand_acc);
+        bump(ctr, C_ALPHA_T, alpha_acc);
+    }
+}
+
+// ------------------------------------------------------------------ tetrahedra
+struct TetArgs {
+    uint64_t n;
+    const float4 *at;
+    const uint32_t *orig;
+    const uint64_t *eoff;
+    const uint32_t *ER;
+    const uint64_t *loff;
+    const uint64_t *link;
+    uint64_t *faces;
+    const uint32_t *cellbeg;
+    const uint32_t *mol;
+    const MolGrid *grids;
+    float alpha;
+    // survivors (as-written) / ordered output (as-run fill)
+    uint2 *surv;          // (ball, packed a | b << 8 | c << 16)
+    uint64_t surv_cap;
+    uint32_t *tcount;     // per ball
+    uint2 *pend;          // tetrahedra waiting for the exact SoS
+    uint64_t pend_cap;
+    const uint64_t *toff; // as-run fill: output offsets per ball
+    uint32_t *tets_out;   // as-run fill: sorted-space vertex quadruples
+    unsigned long long *ctr;
+};
+
+__device__ __forceinline__ void mark_face(uint64_t *F, uint64_t row_base, int W, int a, int b) {
+    atomicOr((unsigned long long *)&F[row_base + (uint64_t)a * W + (b >> 6)],
+             1ull << (b & 63));
+}
+
+// Empty-orthosphere test of one tetrahedron (checkTetsOrthosphere,
+// AlphaComplexLargeData.cu:606-734): 1 = some other ball violates,
+// 2 = none violates but some insphere value is exactly 0 (needs SoS),
+// 0 = empty.
+__device__ __forceinline__ int ortho_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
+                                          uint32_t v2, uint32_t v3, uint32_t v4,
+                                          const Ball a1, const Ball a2, const Ball a3,
+                                          const Ball a4, float4 sphere,
+                                          unsigned long long &evals,
+                                          unsigned long long &oob) {
+    float pa[3], pb[3], pc[3], pd[3], pe[3];
+    float wa, wb, wc, wd, we;
+    pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = a1.r * a1.r;
+    pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
+    pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
+    pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
+    int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
+    int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
+    int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
+    int currCellIndex = lin3(gridX, gridY, gridZ, G.gx, G.gy);
+    float orientation = pac::orient3d(pa, pb, pc, pd);
+    bool zero = false;
+    for (int q = 0; q < 27; q++) {
+        uint32_t beg, end;
+        if (q == 0) {
+            if (currCellIndex < 0 || (uint64_t)currCellIndex >= G.ncell) {
+                oob++;
+                continue;
+            }
+            uint64_t gc = G.cell_base + (uint64_t)currCellIndex;
+            beg = A.cellbeg[gc];
+            end = A.cellbeg[gc + 1];
+        } else {
+            int r = q - 1 + (q >= 14 ? 1 : 0);  // skip the centre (i = j = k = 0)
+            int i = r / 9 - 1, j = (r / 3) % 3 - 1, k = r % 3 - 1;
+            int zz = (int)((unsigned)gridZ + (unsigned)i), yy = (int)((unsigned)gridY + (unsigned)j),
+                xx = (int)((unsigned)gridX + (unsigned)k);
+            if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
+            if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+            uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+            beg = A.cellbeg[gc];
+            end = A.cellbeg[gc + 1];
+        }
+        for (uint32_t e = beg; e < end; e++) {
+            if (e == v1 || e == v2 || e == v3 || e == v4) continue;
+            const Ball atom = pac::ld_ball(&A.at[e]);
+            pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
+            we = atom.r * atom.r;
+            evals++;
+            float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+            if (orientation < 0) {
+                if (result < 0) return 1;
+            } else {
+                if (result > 0) return 1;
+            }
+            if (result == 0) zero = true;
+        }
+    }
+    return zero ? 2 : 0;
+}
+
+// One warp per ball v1.  For each upper neighbour v2 = N[a] the lanes take
+// the alpha triangles (v1, v2, v3 = N[b]); the fourth vertices v4 = N[c]
+// (c > b) are the common bits of rows a and b of v1's link matrix whose
+// face (v2, v3, v4) is also an alpha triangle -- exactly the reference's
+// candidate tetrahedra (AlphaComplexLargeData.cu:350-529).  Each candidate
+// then passes markRealTets and, as written, the empty-orthosphere test.
+// MODE 0: as written, append survivors.  MODE 1: as run, count per ball.
+// MODE 2: as run, write in reference order (needs MODE 1 offsets).
+template <int V, int MODE>
+__global__ void __launch_bounds__(256) k_tets(TetArgs A) {
+    __shared__ uint16_t smap[8][kMaxDeg];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long cand_acc = 0, alpha_acc = 0, evals = 0, oob = 0;
+    for (uint64_t p = warp; p < A.n; p += nwarps) {
+        const uint64_t e0 = A.eoff[p];
+        const int deg = (int)(A.eoff[p + 1] - e0);
+        uint32_t ball_count = 0;
+        if (deg >= 3) {
+            const int W = (deg + 63) >> 6;
+            const uint32_t *N = A.ER + e0;
+            const uint64_t lp = A.loff[p];
+            const uint64_t *Lp = A.link + lp;
+            const Ball B1 = pac::ld_ball(&A.at[p]);
+            const MolGrid G = A.grids[mol_of(A.mol, p)];
+            uint64_t out_base = (MODE == 2) ? A.toff[p] : 0;
+            for (int a = 0; a < deg - 2; a++) {
+                uint64_t ra[kMaxW];
+                int nb = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
+                    nb += __popcll(ra[w]);
+                }
+                if (nb < 2) continue;
+                const uint32_t v2 = __ldg(&N[a]);
+                const uint64_t e2 = A.eoff[v2];
+                const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+                const int W2 = (deg2 + 63) >> 6;
+                const uint64_t l2 = A.loff[v2];
+                const uint64_t *L2 = A.link + l2;
+                for (int c = a + 1 + lane; c < deg; c += 32) {
+                    uint32_t x = __ldg(&N[c]);
+                    int pos = lbound(A.ER + e2, deg2, x);
+                    smap[wib][c] = (pos < deg2 && __ldg(&A.ER[e2 + pos]) == x) ? (uint16_t)pos
+                                                                               : (uint16_t)0xffff;
+                }
+                __syncwarp();
+                const Ball B2 = pac::ld_ball(&A.at[v2]);
+                for (int k0 = 0; k0 < nb; k0 += 32) {
+                    int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
+                    uint32_t lane_cnt = 0;
+                    // MODE 2 needs each lane's count first to place its rows
+                    uint64_t lane_off = 0;
+                    for (int sweep = (MODE == 2 ? 0 : 1); sweep < 2; sweep++) {
+                        if (MODE == 2 && sweep == 1) {
+                            uint32_t incl = lane_cnt;
+                            for (int o = 1; o < 32; o <<= 1) {
+                                uint32_t v = __shfl_up_sync(kFull, incl, o);
+                                if (lane >= o) incl += v;
+                            }
+                            lane_off = out_base + ball_count + (incl - lane_cnt);
+                            ball_count += __shfl_sync(kFull, incl, 31);
+                            lane_cnt = 0;
+                        }
+                        if (b >= 0) {
+                            const uint32_t v3 = __ldg(&N[b]);
+                            const Ball B3 = pac::ld_ball(&A.at[v3]);
+                            const int mb = smap[wib][b];
+                            uint64_t m[kMaxW];
+#pragma unroll
+                            for (int w = 0; w < kMaxW; w++)
+                                m[w] = w < W ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
+                                             : 0;
+                            const uint64_t *R2 = L2 + (uint64_t)mb * W2;
+                            for (int w = 0; w < kMaxW; w++) {
+                                uint64_t bits = m[w];
+                                while (bits) {
+                                    int c = w * 64 + __ffsll((long long)bits) - 1;
+                                    bits &= bits - 1;
+                                    int mc = smap[wib][c];
+                                    if (mb == 0xffff || mc == 0xffff) continue;
+                                    if (!((__ldg(&R2[mc >> 6]) >> (mc & 63)) & 1ull)) continue;
+                                    if (sweep == 1) cand_acc++;
+                                    const uint32_t v4 = __ldg(&N[c]);
+                                    const Ball B4 = pac::ld_ball(&A.at[v4]);
+                                    float4 o;
+                                    if (!pac::tet_alpha(B1, B2, B3, B4, A.alpha, o)) continue;
+                                    if (sweep == 1) alpha_acc++;
+                                    if (MODE == 1) {
+                                        lane_cnt++;
+                                        continue;
+                                    }
+                                    if (MODE == 2) {
+                                        if (sweep == 0) {
+                                            lane_cnt++;
+                                            continue;
+                                        }
+                                        uint64_t q = lane_off + lane_cnt++;
+                                        uint4 t4 = make_uint4((uint32_t)p, v2, v3, v4);
+                                        *(uint4 *)&A.tets_out[4 * q] = t4;
+                                        mark_face(A.faces, lp, W, a, b);
+                                        mark_face(A.faces, lp, W, a, c);
+                                        mark_face(A.faces, lp, W, b, c);
+                                        mark_face(A.faces, l2, W2, mb, mc);
+                                        continue;
+                                    }
+                                    int r = ortho_test(A, G, (uint32_t)p, v2, v3, v4, B1, B2, B3,
+                                                       B4, o, evals, oob);
+                                    if (r == 1) continue;
+                                    uint32_t key = (uint32_t)a | ((uint32_t)b << 8) |
+                                                   ((uint32_t)c << 16);
+                                    if (r == 2) {
+                                        unsigned long long q = atomicAdd(&A.ctr[C_PEND], 1ull);
+                                        if (q < A.pend_cap) A.pend[q] = make_uint2((uint32_t)p, key);
+                                        continue;
+                                    }
+                                    unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
+                                    if (q < A.surv_cap) A.surv[q] = make_uint2((uint32_t)p, key);
+                                    lane_cnt++;
+                                    mark_face(A.faces, lp, W, a, b);
+                                    mark_face(A.faces, lp, W, a, c);
+                                    mark_face(A.faces, lp, W, b, c);
+                                    mark_face(A.faces, l2, W2, mb, mc);
+                                }
+                            }
+                        }
+                    }
+                    if (MODE != 2) {
+                        uint32_t s = lane_cnt;
+                        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+                        ball_count += s;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (lane == 0 && MODE != 2) A.tcount[p] = ball_count;
+    }
+    cand_acc = warp_sum(cand_acc);
+    alpha_acc = warp_sum(alpha_acc);
+    evals = warp_sum(evals);
+    oob = warp_sum(oob);
+    if (lane == 0) {
+        bump(A.ctr, C_CAND_Q, cand_acc);
+        bump(A.ctr, C_ALPHA_Q, alpha_acc);
+        bump(A.ctr, C_INSPHERE, evals);
+        bump(A.ctr, C_OOB, oob);
+    }
+}
+
+// Tetrahedra whose window holds an insphere value of exactly 0: the test
+// again, with the reference's simulation of simplicity for those balls
+// (AlphaComplexLargeData.cu:645-652, 659-667).
+__global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npend) return;
+    uint2 pk = A.pend[t];
+    uint64_t p = pk.x;
+    int a = pk.y & 0xff, b = (pk.y >> 8) & 0xff, c = (pk.y >> 16) & 0xff;
+    const uint64_t e0 = A.eoff[p];
+    const int deg = (int)(A.eoff[p + 1] - e0);
+    const int W = (deg + 63) >> 6;
+    const uint32_t *N = A.ER + e0;
+    uint32_t v[4] = {(uint32_t)p, N[a], N[b], N[c]};
+    Ball B[4];
+    for (int k = 0; k < 4; k++) B[k] = pac::ld_ball(&A.at[v[k]]);
+    float4 sphere;
+    pac::tet_alpha(B[0], B[1], B[2], B[3], A.alpha, sphere);
+    const MolGrid G = A.grids[mol_of(A.mol, p)];
+    float pts[5][3], ws[5];
+    int idx[5];
+    for (int k = 0; k < 4; k++) {
+        pts[k][0] = B[k].x;
+        pts[k][1] = B[k].y;
+        pts[k][2] = B[k].z;
+        ws[k] = B[k].r * B[k].r;
+        idx[k] = (int)A.orig[v[k]] + 1;
+    }
+    float orientation = pac::orient3d(pts[0], pts[1], pts[2], pts[3]);
+    int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
+    int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
+    int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
+    int cc = lin3(gridX, gridY, gridZ, G.gx, G.gy);
+    bool viol = false;
+    for (int q = 0; q < 27 && !viol; q++) {
+        uint32_t beg, end;
+        if (q == 0) {
+            if (cc < 0 || (uint64_t)cc >= G.ncell) continue;
+            beg = A.cellbeg[G.cell_base + cc];
+            end = A.cellbeg[G.cell_base + cc + 1];
+        } else {
+            int r = q - 1 + (q >= 14 ? 1 : 0);
+            int i = r / 9 - 1, j = (r / 3) % 3 - 1, k = r % 3 - 1;
+            int zz = (int)((unsigned)gridZ + (unsigned)i), yy = (int)((unsigned)gridY + (unsigned)j),
+                xx = (int)((unsigned)gridX + (unsigned)k);
+            if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
+            if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+            uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+            beg = A.cellbeg[gc];
+            end = A.cellbeg[gc + 1];
+        }
+        for (uint32_t e = beg; e < end && !viol; e++) {
+            if (e == v[0] || e == v[1] || e == v[2] || e == v[3]) continue;
+            const Ball atom = pac::ld_ball(&A.at[e]);
+            pts[4][0] = atom.x;
+            pts[4][1] = atom.y;
+            pts[4][2] = atom.z;
+            ws[4] = atom.r * atom.r;
+            float result = pac::insphere_w(pts[0], pts[1], pts[2], pts[3], pts[4], ws[0], ws[1],
+                                           ws[2], ws[3], ws[4]);
+            if (result == 0) {
+                idx[4] = (int)A.orig[e] + 1;
+                int status = 0;
+                result = (float)pac::sos_orientation(pts, ws, idx, &status);
+                atomicAdd(&A.ctr[C_SOS], 1ull);
+                if (status == 1) atomicAdd(&A.ctr[C_SOS_RANGE], 1ull);
+            }
+            viol = orientation < 0 ? (result < 0) : (result > 0);
+        }
+    }
+    if (viol) return;
+    unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
+    if (q < A.surv_cap) A.surv[q] = pk;
+    atomicAdd(&A.tcount[p], 1u);
+    const uint64_t lp = A.loff[p];
+    mark_face(A.faces, lp, W, a, b);
+    mark_face(A.faces, lp, W, a, c);
+    mark_face(A.faces, lp, W, b, c);
+    const uint32_t v2 = v[1];
+    const uint64_t e2 = A.eoff[v2];
+    const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+    const int mb = lbound(A.ER + e2, deg2, v[2]), mc = lbound(A.ER + e2, deg2, v[3]);
+    mark_face(A.faces, A.loff[v2], (deg2 + 63) >> 6, mb, mc);
+}
+
+// Survivors to per-ball rows: scatter, then order each ball's rows by
+// (a, b, c) -- the order in which the reference enumerates them.
+__global__ void k_tet_scatter(const uint2 *surv, uint64_t ns, const uint64_t *toff,
+                              uint32_t *cursor, uint32_t *keys) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns) return;
+    uint2 s = surv[t];
+    keys[toff[s.x] + atomicAdd(&cursor[s.x], 1u)] = s.y;
+}
+__global__ void k_tet_sort_emit(uint64_t n, const uint64_t *toff, uint32_t *keys,
+                                const uint64_t *eoff, const uint32_t *ER, const uint32_t *orig,
+                                uint32_t *out) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint64_t b = toff[p], e = toff[p + 1];
+    for (uint64_t i = b + 1; i < e; i++) {
+        uint32_t v = keys[i];
+        uint32_t vk = ((v & 0xff) << 16) | (v & 0xff00) | ((v >> 16) & 0xff);
+        uint64_t j = i;
+        while (j > b) {
+            uint32_t u = keys[j - 1];
+            uint32_t uk = ((u & 0xff) << 16) | (u & 0xff00) | ((u >> 16) & 0xff);
+            if (uk <= vk) break;
+            keys[j] = u;
+            j--;
+        }
+        keys[j] = v;
+    }
+    const uint32_t *N = ER + eoff[p];
+    const uint32_t o1 = orig[p];
+    for (uint64_t i = b; i < e; i++) {
+        uint32_t k = keys[i];
+        uint4 t = make_uint4(o1, orig[N[k & 0xff]], orig[N[(k >> 8) & 0xff]],
+                             orig[N[(k >> 16) & 0xff]]);
+        *(uint4 *)&out[4 * i] = t;
+    }
+}
+__global__ void k_map4(uint64_t nq, const uint32_t *orig, uint32_t *tets) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    uint4 v = *(uint4 *)&tets[4 * t];
+    *(uint4 *)&tets[4 * t] = make_uint4(orig[v.x], orig[v.y], orig[v.z], orig[v.w]);
+}
+
+// ------------------------------------------------------------------ attachment
+// Final triangles of ball i: tetrahedron faces, plus the alpha triangles
+// that are not faces and whose orthosphere no other ball of the 27-cell
+// window reaches (checkDanglingTris, AlphaComplexLargeData.cu:798-872).
+// Also marks the three edges of every final triangle.
+template <int V>
+__global__ void __launch_bounds__(256) k_tri_final(uint64_t n, const float4 *__restrict__ at,
+                                                   const uint64_t *__restrict__ eoff,
+                                                   const uint32_t *__restrict__ ER,
+                                                   const uint64_t *__restrict__ loff,
+                                                   const uint64_t *__restrict__ link,
+                                                   uint64_t *faces, uint32_t *tricount,
+                                                   uint8_t *eflag, const uint32_t *cellbeg,
+                                                   const uint32_t *mol, const MolGrid *grids,
+                                                   float alpha, unsigned long long *ctr) {
+    __shared__ uint64_t sfin[8][kMaxW];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long oob = 0;
+    for (uint64_t p = warp; p < n; p += nwarps) {
+        const uint64_t e0 = eoff[p];
+        const int deg = (int)(eoff[p + 1] - e0);
+        uint32_t count = 0;
+        if (deg >= 2) {
+            const int W = (deg + 63) >> 6;
+            const uint32_t *N = ER + e0;
+            const uint64_t lp = loff[p];
+            const Ball A0 = pac::ld_ball(&at[p]);
+            const MolGrid G = grids[mol_of(mol, p)];
+            for (int a = 0; a < deg - 1; a++) {
+                uint64_t la[kMaxW], fa[kMaxW], cand[kMaxW];
+                int nc = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    la[w] = w < W ? link[lp + (uint64_t)a * W + w] : 0;
+                    fa[w] = w < W ? faces[lp + (uint64_t)a * W + w] : 0;
+                    cand[w] = la[w] & ~fa[w];
+                    nc += __popcll(cand[w]);
+                }
+                if (!__any_sync(kFull, (la[0] | la[1] | la[2] | la[3]) != 0)) continue;
+                if (lane < kMaxW) sfin[wib][lane] = lane < W ? faces[lp + (uint64_t)a * W + lane] : 0;
+                __syncwarp();
+                const uint32_t v1 = N[a];
+                const Ball A1 = pac::ld_ball(&at[v1]);
+                for (int k0 = 0; k0 < nc; k0 += 32) {
+                    int b = (k0 + lane < nc) ? select_bit(cand, W, k0 + lane) : -1;
+                    bool keep = false;
+                    if (b >= 0) {
+                        const uint32_t v2 = N[b];
+                        float4 p1;
+                        pac::tri_alpha<V>(A0, A1, pac::ld_ball(&at[v2]), alpha, p1);
+                        float currentDist = p1.w;
+                        int gridX = pac::cell_coord(p1.x, G.minx, G.step);
+                        int gridY = pac::cell_coord(p1.y, G.miny, G.step);
+                        int gridZ = pac::cell_coord(p1.z, G.minz, G.step);
+                        int cc = lin3(gridX, gridY, gridZ, G.gx, G.gy);
+                        bool att = false;
+                        for (int q = 0; q < 27 && !att; q++) {
+                            uint32_t beg, end;
+                            if (q == 0) {
+                                if (cc < 0 || (uint64_t)cc >= G.ncell) {
+                                    oob++;
+                                    continue;
+                                }
+                                beg = cellbeg[G.cell_base + cc];
+                                end = cellbeg[G.cell_base + cc + 1];
+                            } else {
+                                int r = q - 1 + (q >= 14 ? 1 : 0);
+                                int i = r / 9 - 1, j = (r / 3) % 3 - 1, k = r % 3 - 1;
+                                int zz = (int)((unsigned)gridZ + (unsigned)i),
+                                    yy = (int)((unsigned)gridY + (unsigned)j),
+                                    xx = (int)((unsigned)gridX + (unsigned)k);
+                                if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
+                                if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+                                uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+                                beg = cellbeg[gc];
+                                end = cellbeg[gc + 1];
+                            }
+                            for (uint32_t e = beg; e < end; e++) {
+                                if (e == p || e == v1 || e == v2) continue;
+                                if (pac::attached(pac::ld_ball(&at[e]), p1.x, p1.y, p1.z,
+                                                  currentDist)) {
+                                    att = true;
+                                    break;
+                                }
+                            }
+                        }
+                        keep = !att;
+                    }
+                    if (keep) atomicOr((unsigned long long *)&sfin[wib][b >> 6], 1ull << (b & 63));
+                }
+                __syncwarp();
+                // final row: write, count, and mark the edges of its triangles
+                uint64_t fin[kMaxW];
+                int nf = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    fin[w] = sfin[wib][w];
+                    nf += __popcll(fin[w]);
+                }
+                __syncwarp();
+                if (lane < W) faces[lp + (uint64_t)a * W + lane] = fin[lane];
+                count += nf;
+                if (nf) {
+                    if (lane == 0) eflag[e0 + a] = 1;
+                    const uint64_t e1 = eoff[v1];
+                    const int deg1 = (int)(eoff[v1 + 1] - e1);
+                    for (int k0 = 0; k0 < nf; k0 += 32) {
+                        int b = (k0 + lane < nf) ? select_bit(fin, W, k0 + lane) : -1;
+                        if (b >= 0) {
+                            eflag[e0 + b] = 1;
+                            const uint32_t v2 = N[b];
+                            int pos = lbound(ER + e1, deg1, v2);
+                            if (pos < deg1 && ER[e1 + pos] == v2) eflag[e1 + pos] = 1;
+                        }
+                    }
+                }
+            }
+        }
+        if (lane == 0) tricount[p] = count;
+    }
+    oob = warp_sum(oob);
+    if (lane == 0) bump(ctr, C_OOB, oob);
+}
+
+// Final edges: edges of final triangles, plus the alpha edges whose radical
+// foot no other ball reaches (checkDanglingEdges, AlphaComplexLargeData.cu:924-1011).
+template <int V>
+__global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__restrict__ at,
+                                                    const uint64_t *__restrict__ eoff,
+                                                    const uint32_t *__restrict__ ER,
+                                                    uint8_t *eflag, const uint32_t *cellbeg,
+                                                    const uint32_t *mol, const MolGrid *grids,
+                                                    unsigned long long *ctr) {
+    const int lane = threadIdx.x & 31;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long oob = 0;
+    for (uint64_t p = warp; p < n; p += nwarps) {
+        const uint64_t e0 = eoff[p];
+        const int deg = (int)(eoff[p + 1] - e0);
+        if (!deg) continue;
+        const Ball a1 = pac::ld_ball(&at[p]);
+        const MolGrid G = grids[mol_of(mol, p)];
+        for (int k = lane; k < deg; k += 32) {
+            if (eflag[e0 + k]) continue;
+            const uint32_t v2 = ER[e0 + k];
+            float px, py, pz, currentDist;
+            pac::edge_foot(a1, pac::ld_ball(&at[v2]), px, py, pz, currentDist);
+            int gridX = pac::cell_coord(px, G.minx, G.step);
+            int gridY = pac::cell_coord(py, G.miny, G.step);
+            int gridZ = pac::cell_coord(pz, G.minz, G.step);
+            int cc = lin3(gridX, gridY, gridZ, G.gx, G.gy);
+            bool att = false;
+            for (int q = 0; q < 27 && !att; q++) {
+                uint32_t beg, end;
+                if (q == 0) {
+                    if (cc < 0 || (uint64_t)cc >= G.ncell) {
+                        oob++;
+                        continue;
+                    }
+                    beg = cellbeg[G.cell_base + cc];
+                    end = cellbeg[G.cell_base + cc + 1];
+                } else {
+                    int r = q - 1 + (q >= 14 ? 1 : 0);
+                    int i = r / 9 - 1, j = (r / 3) % 3 - 1, kk = r % 3 - 1;
+                    int zz = (int)((unsigned)gridZ + (unsigned)i),
+                        yy = (int)((unsigned)gridY + (unsigned)j),
+                        xx = (int)((unsigned)gridX + (unsigned)kk);
+                    if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
+                    if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+                    uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+                    beg = cellbeg[gc];
+                    end = cellbeg[gc + 1];
+                }
+                for (uint32_t e = beg; e < end; e++) {
+                    if (e == p || e == v2) continue;
+                    if (pac::attached(pac::ld_ball(&at[e]), px, py, pz, currentDist)) {
+                        att = true;
+                        break;
+                    }
+                }
+            }
+            if (!att) eflag[e0 + k] = 1;
+        }
+    }
+    oob = warp_sum(oob);
+    if (lane == 0) bump(ctr, C_OOB, oob);
+}
+
+// ------------------------------------------------------------------ emission
+__global__ void k_emit_edges(uint64_t n, const uint64_t *eoff, const uint32_t *ER,
+                             const uint8_t *eflag, const uint64_t *epos, const uint32_t *orig,
+                             uint32_t *out) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    uint32_t o = orig[p];
+    for (uint64_t k = eoff[p]; k < eoff[p + 1]; k++)
+        if (eflag[k]) {
+            uint64_t q = epos[k];
+            out[2 * q] = o;
+            out[2 * q + 1] = orig[ER[k]];
+        }
+}
+__global__ void __launch_bounds__(256) k_emit_tris(uint64_t n, const uint64_t *eoff,
+                                                   const uint32_t *ER, const uint64_t *loff,
+                                                   const uint64_t *faces, const uint64_t *tpos,
+                                                   const uint32_t *orig, uint32_t *out) {
+    const int lane = threadIdx.x & 31;
+    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t p = warp; p < n; p += nwarps) {
+        const int deg = (int)(eoff[p + 1] - eoff[p]);
+        if (deg < 2) continue;
+        const int W = (deg + 63) >> 6;
+        const uint32_t *N = ER + eoff[p];
+        const uint32_t o0 = orig[p];
+        uint64_t q = tpos[p];
+        for (int a = 0; a < deg - 1; a++) {
+            uint64_t f[kMaxW];
+            int nf = 0;
+            for (int w = 0; w < kMaxW; w++) {
+                f[w] = w < W ? faces[loff[p] + (uint64_t)a * W + w] : 0;
+                nf += __popcll(f[w]);
+            }
+            const uint32_t o1 = orig[N[a]];
+            for (int k0 = 0; k0 < nf; k0 += 32) {
+                int k = k0 + lane;
+                if (k < nf) {
+                    int b = select_bit(f, W, k);
+                    out[3 * (q + k)] = o0;
+                    out[3 * (q + k) + 1] = o1;
+                    out[3 * (q + k) + 2] = orig[N[b]];
+                }
+            }
+            q += nf;
+        }
+    }
+}
+// first output row of every molecule (and the totals at m = n_mol)
+__global__ void k_mol_rows(uint32_t n_mol, const uint64_t *ball_off, uint64_t n,
+                           const uint64_t *eoff, const uint64_t *epos, const uint64_t *tpos,
+                           const uint64_t *toff, uint64_t *rows) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m > n_mol) return;
+    uint64_t b = m < n_mol ? ball_off[m] : n;
+    rows[m] = epos[eoff[b]];
+    rows[(n_mol + 1) + m] = tpos[b];
+    rows[2 * (n_mol + 1) + m] = toff[b];
+}
+
+// ------------------------------------------------------------------ host
+struct Timer {
+    pac::Ctx &ctx;
+    int i = 0;
+    explicit Timer(pac::Ctx &c) : ctx(c) {}
+    void mark() {
+        if (i < 16) cudaEventRecord(ctx.ev[i++], ctx.stream);
+    }
+    double ms(int a, int b) {
+        float f = 0;
+        if (a < i && b < i) cudaEventElapsedTime(&f, ctx.ev[a], ctx.ev[b]);
+        return f;
+    }
+};
+
+static unsigned blocks_for(uint64_t n, unsigned threads) {
+    uint64_t b = (n + threads - 1) / threads;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, 0x7fffffffu));
+}
+static unsigned warp_blocks(uint64_t items) {
+    // 8 warps per block, grid-stride: enough blocks to fill 148 SMs many times
+    uint64_t b = (items + 7) / 8;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 64));
+}
+
+template <int V>
+static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
+                      pac::PassOutput &out, pac_stats *st) {
+    cudaStream_t s = ctx.stream;
+    pac::Arena &ar = ctx.arena;
+    const uint64_t n = in.n;
+    const uint32_t nm = in.n_mol;
+    Timer tm(ctx);
+    tm.mark();  // 0
+
+    unsigned long long *ctr = ar.alloc_n<unsigned long long>(C_NCOUNTERS);
+    int *mm = ar.alloc_n<int>(8 * (size_t)nm);
+    MolGrid *grids = ar.alloc_n<MolGrid>(nm);
+    uint64_t *ncell_d = ar.alloc_n<uint64_t>(nm);
+    uint64_t *d_off = ar.alloc_n<uint64_t>(nm + 1);
+    uint32_t *mol = nullptr;
+    if (!ctr || !mm || !grids || !ncell_d || !d_off) return PAC_ERR_OOM;
+    CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
+    {
+        std::vector<int> init(8 * (size_t)nm);
+        for (uint32_t m = 0; m < nm; m++)
+            for (int q = 0; q < 4; q++) {
+                init[8 * m + q] = 0x7fffffff;
+                init[8 * m + 4 + q] = (int)0x80000000;
+            }
+        CK(cudaMemcpyAsync(mm, init.data(), sizeof(int) * init.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_off, in.h_offsets, sizeof(uint64_t) * (nm + 1),
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));  // `init` leaves scope
+    }
+    if (nm > 1) {
+        mol = ar.alloc_n<uint32_t>(n);
+        if (!mol) return PAC_ERR_OOM;
+        k_mol_ids<<<nm, 256, 0, s>>>(d_off, nm, mol);
+        LAUNCH_CHECK(ctx);
+    }
+    k_bbox<<<blocks_for(n, 256), 256, 0, s>>>(in.d_balls, n, mol, mm);
+    LAUNCH_CHECK(ctx);
+    k_grid<<<blocks_for(nm, 128), 128, 0, s>>>(mm, nm, in.alpha, grids, ncell_d);
+    LAUNCH_CHECK(ctx);
+    std::vector<MolGrid> hg(nm);
+    CK(cudaMemcpyAsync(hg.data(), grids, sizeof(MolGrid) * nm, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    uint64_t total_cells = 0;
+    for (uint32_t m = 0; m < nm; m++) {
+        if (hg[m].gx <= 0 || hg[m].gy <= 0 || hg[m].gz <= 0 || hg[m].ncell > 0x7fffffffull)
+            return pac::set_error(PAC_ERR_CAPACITY,
+                                  "grid of molecule " + std::to_string(m) +
+                                      " exceeds the reference's int cell index range");
+        hg[m].cell_base = total_cells;
+        hg[m].atom_base = in.h_offsets[m];
+        total_cells += hg[m].ncell;
+    }
+    if (total_cells >= 0xffffffffull)
+        return pac::set_error(PAC_ERR_CAPACITY, "more than 2^32 cells in one pass");
+    CK(cudaMemcpyAsync(grids, hg.data(), sizeof(MolGrid) * nm, cudaMemcpyHostToDevice, s));
+
+    // ---- binning
+    uint32_t *gcell = ar.alloc_n<uint32_t>(n), *slot = ar.alloc_n<uint32_t>(n);
+    uint32_t *cellcnt = ar.alloc_n<uint32_t>(total_cells);
+    uint32_t *cellbeg = ar.alloc_n<uint32_t>(total_cells + 1);
+    uint32_t *perm = ar.alloc_n<uint32_t>(n);
+    float4 *at = ar.alloc_n<float4>(n);
+    uint32_t *orig = ar.alloc_n<uint32_t>(n), *cellof = ar.alloc_n<uint32_t>(n);
+    if (!gcell || !slot || !cellcnt || !cellbeg || !perm || !at || !orig || !cellof)
+        return PAC_ERR_OOM;
+    CK(cudaMemsetAsync(cellcnt, 0, sizeof(uint32_t) * total_cells, s));
+    k_cellkey<<<blocks_for(n, 256), 256, 0, s>>>(in.d_balls, n, mol, grids, gcell, slot, cellcnt);
+    LAUNCH_CHECK(ctx);
+    int rc = exclusive_scan(ctx, cellcnt, total_cells, cellbeg);
+    if (rc) return rc;
+    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, gcell, slot, cellbeg, perm);
+    LAUNCH_CHECK(ctx);
+    k_cellsort<<<blocks_for(total_cells, 256), 256, 0, s>>>(total_cells, cellbeg, perm);
+    LAUNCH_CHECK(ctx);
+    k_gather<<<blocks_for(n, 256), 256, 0, s>>>(n, perm, in.d_balls, in.sol, gcell, mol, grids,
+                                                at, orig, cellof);
+    LAUNCH_CHECK(ctx);
+    tm.mark();  // 1
+
+    // ---- alpha edges
+    uint32_t *ecount = ar.alloc_n<uint32_t>(n);
+    uint64_t *eoff = ar.alloc_n<uint64_t>(n + 1);
+    if (!ecount || !eoff) return PAC_ERR_OOM;
+    k_edges<V, false><<<warp_blocks(n), 256, 0, s>>>(n, at, cellof, cellbeg, mol, grids, in.alpha,
+                                                     ecount, nullptr, nullptr, ctr);
+    LAUNCH_CHECK(ctx);
+    rc = exclusive_scan(ctx, ecount, n, eoff);
+    if (rc) return rc;
+    uint64_t nE = 0;
+    CK(cudaMemcpyAsync(&nE, eoff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    uint32_t *ER = ar.alloc_n<uint32_t>(nE);
+    uint8_t *eflag = ar.alloc_n<uint8_t>(nE);
+    uint64_t *lsize = ar.alloc_n<uint64_t>(n), *loff = ar.alloc_n<uint64_t>(n + 1);
+    if (!ER || !eflag || !lsize || !loff) return PAC_ERR_OOM;
+    k_edges<V, true><<<warp_blocks(n), 256, 0, s>>>(n, at, cellof, cellbeg, mol, grids, in.alpha,
+                                                    nullptr, eoff, ER, ctr);
+    LAUNCH_CHECK(ctx);
+    CK(cudaMemsetAsync(eflag, 0, nE ? nE : 1, s));
+    k_link_size<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, lsize, ctr);
+    LAUNCH_CHECK(ctx);
+    rc = exclusive_scan(ctx, lsize, n, loff);
+    if (rc) return rc;
+    uint64_t nL = 0;
+    unsigned long long maxdeg = 0;
+    CK(cudaMemcpyAsync(&nL, loff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&maxdeg, ctr + C_MAXDEG, sizeof(maxdeg), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (maxdeg > (unsigned long long)kMaxDeg)
+        return pac::set_error(PAC_ERR_CAPACITY, "a ball has " + std::to_string(maxdeg) +
+                                                    " alpha edges to higher balls; the limit is " +
+                                                    std::to_string(kMaxDeg));
+    tm.mark();  // 2
+
+    // ---- alpha triangles (link matrices)
+    uint64_t *link = ar.alloc_n<uint64_t>(nL), *faces = ar.alloc_n<uint64_t>(nL);
+    if (!link || !faces) return PAC_ERR_OOM;
+    CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
+    k_link<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, loff, link, in.alpha, ctr);
+    LAUNCH_CHECK(ctx);
+    tm.mark();  // 3
+
+    // ---- tetrahedra
+    TetArgs T{};
+    T.n = n;
+    T.at = at;
+    T.orig = orig;
+    T.eoff = eoff;
+    T.ER = ER;
+    T.loff = loff;
+    T.link = link;
+    T.faces = faces;
+    T.cellbeg = cellbeg;
+    T.mol = mol;
+    T.grids = grids;
+    T.alpha = in.alpha;
+    T.ctr = ctr;
+    T.tcount = ar.alloc_n<uint32_t>(n);
+    uint64_t *toff = ar.alloc_n<uint64_t>(n + 1);
+    if (!T.tcount || !toff) return PAC_ERR_OOM;
+    uint64_t nQ = 0;
+    uint32_t *tets_sorted = nullptr;
+    if (cfg.tet_mode == PAC_TETS_AS_RUN) {
+        k_tets<V, 1><<<warp_blocks(n), 256, 0, s>>>(T);
+        LAUNCH_CHECK(ctx);
+        rc = exclusive_scan(ctx, T.tcount, n, toff);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(&nQ, toff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        tets_sorted = ar.alloc_n<uint32_t>(4 * nQ);
+        if (!tets_sorted) return PAC_ERR_OOM;
+        T.toff = toff;
+        T.tets_out = tets_sorted;
+        // the second sweep counts candidates again: reset those counters
+        CK(cudaMemsetAsync(ctr + C_CAND_Q, 0, 2 * sizeof(unsigned long long), s));
+        k_tets<V, 2><<<warp_blocks(n), 256, 0, s>>>(T);
+        LAUNCH_CHECK(ctx);
+    } else {
+        uint64_t cap = std::max<uint64_t>(1024, 16 * n);
+        for (int attempt = 0; attempt < 2; attempt++) {
+            T.surv = ar.alloc_n<uint2>(cap);
+            T.surv_cap = cap;
+            T.pend = ar.alloc_n<uint2>(cap / 4 + 1024);
+            T.pend_cap = cap / 4 + 1024;
+            if (!T.surv || !T.pend) return PAC_ERR_OOM;
+            CK(cudaMemsetAsync(ctr + C_CAND_Q, 0, 2 * sizeof(unsigned long long), s));
+            CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
+            CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
+            CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
+            k_tets<V, 0><<<warp_blocks(n), 256, 0, s>>>(T);
+            LAUNCH_CHECK(ctx);
+            unsigned long long sp[2];
+            CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(sp), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            uint64_t need = std::max<uint64_t>(sp[0] + sp[1], 4 * sp[1]);
+            if (sp[0] + sp[1] <= cap && sp[1] <= T.pend_cap) {
+                if (sp[1]) {
+                    k_sos_resolve<<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
+                    LAUNCH_CHECK(ctx);
+                    CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(unsigned long long),
+                                       cudaMemcpyDeviceToHost, s));
+                    CK(cudaStreamSynchronize(s));
+                }
+                nQ = sp[0];
+                break;
+            }
+            if (attempt == 1)
+                return pac::set_error(PAC_ERR_CAPACITY, "tetrahedron buffer overflow");
+            cap = need + 1024;
+        }
+        rc = exclusive_scan(ctx, T.tcount, n, toff);
+        if (rc) return rc;
+    }
+    tm.mark();  // 4
+
+    // ---- final triangles and edges
+    uint32_t *tricount = ar.alloc_n<uint32_t>(n);
+    uint64_t *tpos = ar.alloc_n<uint64_t>(n + 1);
+    uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
+    if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
+    k_tri_final<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, loff, link, faces, tricount,
+                                                  eflag, cellbeg, mol, grids, in.alpha, ctr);
+    LAUNCH_CHECK(ctx);
+    tm.mark();  // 5
+    k_edge_final<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, eflag, cellbeg, mol, grids,
+                                                   ctr);
+    LAUNCH_CHECK(ctx);
+    tm.mark();  // 6
+
+    // ---- emission
+    rc = exclusive_scan(ctx, tricount, n, tpos);
+    if (rc) return rc;
+    rc = exclusive_scan(ctx, eflag, nE, epos);
+    if (rc) return rc;
+    uint64_t nT = 0, nEf = 0;
+    CK(cudaMemcpyAsync(&nT, tpos + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&nEf, epos + nE, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    out.d_edges = ar.alloc_n<uint32_t>(2 * nEf);
+    out.d_tris = ar.alloc_n<uint32_t>(3 * nT);
+    out.d_tets = ar.alloc_n<uint32_t>(4 * nQ);
+    if (!out.d_edges || !out.d_tris || !out.d_tets) return PAC_ERR_OOM;
+    k_emit_edges<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, ER, eflag, epos, orig, out.d_edges);
+    LAUNCH_CHECK(ctx);
+    k_emit_tris<<<warp_blocks(n), 256, 0, s>>>(n, eoff, ER, loff, faces, tpos, orig, out.d_tris);
+    LAUNCH_CHECK(ctx);
+    if (cfg.tet_mode == PAC_TETS_AS_RUN) {
+        CK(cudaMemcpyAsync(out.d_tets, tets_sorted, sizeof(uint32_t) * 4 * (nQ ? nQ : 1),
+                           cudaMemcpyDeviceToDevice, s));
+        k_map4<<<blocks_for(nQ, 256), 256, 0, s>>>(nQ, orig, out.d_tets);
+        LAUNCH_CHECK(ctx);
+    } else {
+        uint32_t *cursor = ar.alloc_n<uint32_t>(n), *keys = ar.alloc_n<uint32_t>(nQ);
+        if (!cursor || !keys) return PAC_ERR_OOM;
+        CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * n, s));
+        k_tet_scatter<<<blocks_for(nQ, 256), 256, 0, s>>>(T.surv, nQ, toff, cursor, keys);
+        LAUNCH_CHECK(ctx);
+        k_tet_sort_emit<<<blocks_for(n, 128), 128, 0, s>>>(n, toff, keys, eoff, ER, orig,
+                                                           out.d_tets);
+        LAUNCH_CHECK(ctx);
+    }
+    out.n_edges = nEf;
+    out.n_tris = nT;
+    out.n_tets = nQ;
+    // per-molecule row offsets
+    out.edge_off.assign(nm + 1, 0);
+    out.tri_off.assign(nm + 1, 0);
+    out.tet_off.assign(nm + 1, 0);
+    if (nm == 1) {
+        out.edge_off[1] = nEf;
+        out.tri_off[1] = nT;
+        out.tet_off[1] = nQ;
+    } else {
+        uint64_t *rows = ar.alloc_n<uint64_t>(3 * (size_t)(nm + 1));
+        if (!rows) return PAC_ERR_OOM;
+        k_mol_rows<<<blocks_for(nm + 1, 128), 128, 0, s>>>(nm, d_off, n, eoff, epos, tpos, toff,
+                                                          rows);
+        LAUNCH_CHECK(ctx);
+        std::vector<uint64_t> h(3 * (size_t)(nm + 1));
+        CK(cudaMemcpyAsync(h.data(), rows, sizeof(uint64_t) * h.size(), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (uint32_t m = 0; m <= nm; m++) {
+            out.edge_off[m] = h[m];
+            out.tri_off[m] = h[(nm + 1) + m];
+            out.tet_off[m] = h[2 * (nm + 1) + m];
+        }
+    }
+    tm.mark();  // 7
+    unsigned long long hc[C_NCOUNTERS];
+    CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hc[C_SOS_RANGE])
+        return pac::set_error(PAC_ERR_EXACT_RANGE,
+                              "coordinate range too wide for the exact SoS integers");
+    if (st) {
+        st->n_balls = n;
+        st->n_cells = total_cells;
+        st->cand_edges = hc[C_CAND_E];
+        st->alpha_edges = hc[C_ALPHA_E];
+        st->cand_tris = hc[C_CAND_T];
+        st->alpha_tris = hc[C_ALPHA_T];
+        st->cand_tets = hc[C_CAND_Q];
+        st->alpha_tets = hc[C_ALPHA_Q];
+        st->final_edges = nEf;
+        st->final_tris = nT;
+        st->final_tets = nQ;
+        st->insphere_evals = hc[C_INSPHERE];
+        st->sos_calls = hc[C_SOS];
+        st->ortho_out_of_grid = hc[C_OOB];
+        st->max_degree = maxdeg;
+        st->ms_grid = tm.ms(0, 1);
+        st->ms_edges = tm.ms(1, 2);
+        st->ms_tris = tm.ms(2, 3);
+        st->ms_tets = tm.ms(3, 4);
+        st->ms_tri_attach = tm.ms(4, 5);
+        st->ms_edge_attach = tm.ms(5, 6);
+        st->ms_emit = tm.ms(6, 7);
+        if (nm == 1) {
+            st->grid[0] = hg[0].gx;
+            st->grid[1] = hg[0].gy;
+            st->grid[2] = hg[0].gz;
+            st->step = hg[0].step;
+        }
+    }
+    return PAC_OK;
+}
+
+int run_pass(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
+             pac::PassOutput &out, pac_stats *st) {
+    if (cfg.formula == PAC_FORMULA_PLAIN_XMP) return run_pass_v<pac::kPlainXmp>(ctx, cfg, in, out, st);
+    return run_pass_v<pac::kUpstream>(ctx, cfg, in, out, st);
+}
+
+}  // namespace PAC_NS

@@ -1,0 +1,227 @@
+"""GPU parity tests: the CUDA engine, called through the C ABI, against the
+reference's shipped outputs and against the CPU restatement, bit for bit
+and in the reference binary's output order."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, canonical, golden
+
+pytestmark = pytest.mark.gpu
+
+FORMULA = {0: "upstream", 1: "plain-xmp"}
+
+
+def _engine(pac, formula=0, tet_mode="as-written", predicates="strict"):
+    return pac.Engine(device=0, formula=FORMULA[formula], tet_mode=tet_mode, predicates=predicates)
+
+
+def _same(res, E, T, Q):
+    np.testing.assert_array_equal(res.edges, E)
+    np.testing.assert_array_equal(res.tris, T)
+    np.testing.assert_array_equal(res.tets, Q)
+
+
+# ------------------------------------------------------------ shipped outputs
+@pytest.mark.parametrize("name,formula", [("1grm_ld_alpha1", 0), ("1grm_plain_alpha1", 1)])
+def test_golden_outputs_as_run(pac, name, formula):
+    balls, E, T, Q = golden(name)
+    with _engine(pac, formula, "as-run") as eng:
+        _same(eng.alpha_complex(balls, 0.0, 1.0), E, T, Q)
+
+
+def test_golden_1k4c_against_restatement(pac, orc):
+    balls, E, T, Q = golden("1k4c_plain_alpha1")
+    for mode, flag in (("as-run", False), ("as-written", True)):
+        e, t, q, _ = orc.alpha_complex(balls, 0.0, 1.0, orc.PLAIN_XMP, tet_ortho=flag)
+        with _engine(pac, 1, mode) as eng:
+            _same(eng.alpha_complex(balls, 0.0, 1.0), e, t, q)
+
+
+# ------------------------------------------------------------ synthetic cases
+CASES = [
+    # n, seed offset, sol, alpha, snapped
+    (300, 0, 0.0, 0.0, False),
+    (1300, 0, 0.0, 0.0, False),      # the 1,300-ball plain case
+    (1300, 0, 1.4, 1.0, False),
+    (2000, 1, 1.4, 1.0, True),       # lattice-snapped: exact zeros, SoS
+    (3000, 7, 1.4, 0.5, False),
+    (800, 9, 0.5, 2.0, True),
+]
+
+
+@pytest.mark.parametrize("n,seed,sol,alpha,snap", CASES)
+@pytest.mark.parametrize("formula", [0, 1])
+def test_synthetic_against_restatement(pac, orc, n, seed, sol, alpha, snap, formula):
+    balls = (pac.snapped_globule(n, seed=pac.SEED_BASE + seed) if snap
+             else pac.globule(n, seed=pac.SEED_BASE + seed))
+    for mode, flag in (("as-written", True), ("as-run", False)):
+        if mode == "as-run" and n > 2000 and sol > 0:
+            continue  # as-run output grows ~2700 tetrahedra per ball
+        e, t, q, st = orc.alpha_complex(balls, sol, alpha, formula, tet_ortho=flag)
+        with _engine(pac, formula, mode) as eng:
+            r = eng.alpha_complex(balls, sol, alpha)
+        _same(r, e, t, q)
+        for k in ("cand_edges", "alpha_edges", "cand_tris", "alpha_tris", "cand_tets",
+                  "alpha_tets"):
+            assert r.stats[k] == st[k], k
+        if flag:
+            assert r.stats["sos_calls"] == st["sos_calls"]
+
+
+@pytest.mark.slow
+def test_degenerate_25k_as_written(pac, orc):
+    """The 25,000-ball lattice-snapped stress case (sol 1.4, alpha 1)."""
+    balls = pac.snapped_globule(25000, seed=pac.SEED_BASE + 1)
+    e, t, q, st = orc.alpha_complex(balls, 1.4, 1.0, orc.UPSTREAM, tet_ortho=True)
+    with _engine(pac, 0, "as-written") as eng:
+        r = eng.alpha_complex(balls, 1.4, 1.0)
+    _same(r, e, t, q)
+    assert st["sos_calls"] > 0 and r.stats["sos_calls"] == st["sos_calls"]
+
+
+# ------------------------------------------------------------ edge cases
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5])
+def test_tiny_inputs(pac, orc, n):
+    balls = np.array([[0, 0, 0, 1.7], [1.5, 0, 0, 1.6], [0.4, 1.3, 0, 1.5],
+                      [0.5, 0.5, 1.2, 1.8], [1.1, 1.0, 1.1, 1.52]], np.float32)[:n]
+    for mode, flag in (("as-written", True), ("as-run", False)):
+        with _engine(pac, 0, mode) as eng:
+            r = eng.alpha_complex(balls, 1.4, 1.0)
+        if n == 0:
+            assert r.counts() == (0, 0, 0)
+            continue
+        e, t, q, _ = orc.alpha_complex(balls, 1.4, 1.0, 0, tet_ortho=flag)
+        _same(r, e, t, q)
+
+
+def test_coplanar_and_cospherical_lattice(pac, orc):
+    """All centres on a 1 A cubic lattice with equal radii: every insphere
+    test is degenerate somewhere, SoS decides."""
+    g = np.stack(np.meshgrid(np.arange(6), np.arange(6), np.arange(4), indexing="ij"), -1)
+    balls = np.concatenate([g.reshape(-1, 3), np.full((g.size // 3, 1), 1.5)], 1).astype(np.float32)
+    for formula in (0, 1):
+        e, t, q, st = orc.alpha_complex(balls, 0.0, 0.5, formula, tet_ortho=True)
+        with _engine(pac, formula, "as-written") as eng:
+            r = eng.alpha_complex(balls, 0.0, 0.5)
+        _same(r, e, t, q)
+        assert st["sos_calls"] > 0
+
+
+def test_far_apart_and_duplicate_free_sparse(pac, orc):
+    rng = np.random.default_rng(3)
+    balls = np.concatenate([rng.uniform(-300, 300, (200, 3)), np.full((200, 1), 1.7)], 1)
+    balls = balls.astype(np.float32)
+    e, t, q, _ = orc.alpha_complex(balls, 1.4, 1.0, 0, tet_ortho=True)
+    with _engine(pac, 0) as eng:
+        _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
+
+
+def test_non_finite_input_rejected(pac):
+    balls = np.array([[0, 0, 0, 1.7], [np.nan, 0, 0, 1.6]], np.float32)
+    with _engine(pac) as eng:
+        with pytest.raises(pac.PacError) as ei:
+            eng.alpha_complex(balls, 1.4, 1.0)
+        assert ei.value.status == -1
+        # the context stays usable
+        r = eng.alpha_complex(balls[:1], 1.4, 1.0)
+        assert r.counts() == (0, 0, 0)
+
+
+def test_degree_limit_reported(pac):
+    """A clump denser than any molecule exceeds the supported upper degree:
+    a clear capacity error, and the context stays usable."""
+    rng = np.random.default_rng(1)
+    balls = np.concatenate([rng.uniform(0, 4, (600, 3)), np.full((600, 1), 1.7)], 1)
+    with _engine(pac) as eng:
+        with pytest.raises(pac.PacError) as ei:
+            eng.alpha_complex(balls.astype(np.float32), 1.4, 1.0)
+        assert ei.value.status == -3
+        r = eng.alpha_complex(pac.globule(300), 1.4, 1.0)
+        assert r.counts()[0] > 0
+
+
+def test_deterministic_reruns(pac):
+    balls = pac.globule(5000, seed=99)
+    with _engine(pac) as eng:
+        a = eng.alpha_complex(balls, 1.4, 1.0)
+        b = eng.alpha_complex(balls, 1.4, 1.0)
+    _same(a, b.edges, b.tris, b.tets)
+
+
+# ------------------------------------------------------------ batched mode
+def test_batch_equals_per_molecule(pac):
+    sizes = np.array([250, 1, 0, 700, 1200, 3, 400], np.uint32)
+    balls, off = pac.batch(sizes, seed=77)
+    with _engine(pac) as eng:
+        res, st = eng.alpha_complex_batch(balls, off, 1.4, 0.5)
+        assert len(res) == len(sizes)
+        for m in range(len(sizes)):
+            single = eng.alpha_complex(balls[off[m]:off[m + 1]], 1.4, 0.5)
+            _same(res[m], single.edges, single.tris, single.tets)
+
+
+# ------------------------------------------------------------ device API
+class _DeviceView:
+    """__cuda_array_interface__ over a raw device pointer (uint32)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4",
+                                         "data": (ptr, True), "version": 2}
+
+
+def _device_list(ptr, rows, k):
+    import ctypes
+    import torch
+    if rows == 0:
+        return np.zeros((0, k), np.uint32)
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    t = torch.as_tensor(_DeviceView(addr, rows * k), device="cuda")
+    return t.cpu().numpy().view(np.uint32).reshape(rows, k)
+
+
+def test_device_entry_point(pac):
+    import torch
+    balls = pac.globule(2000, seed=4)
+    with _engine(pac) as eng:
+        host = eng.alpha_complex(balls, 1.4, 1.0)
+        d = torch.from_numpy(balls).cuda()
+        cx, st = eng.alpha_complex_device(d.data_ptr(), len(balls), 1.4, 1.0)
+        assert cx.on_device == 1 and st["kernels_launched"] > 0
+        np.testing.assert_array_equal(_device_list(cx.edges, cx.n_edges, 2), host.edges)
+        np.testing.assert_array_equal(_device_list(cx.tris, cx.n_tris, 3), host.tris)
+        np.testing.assert_array_equal(_device_list(cx.tets, cx.n_tets, 4), host.tets)
+
+
+# ------------------------------------------------------------ CLI
+def test_cli_reproduces_golden_file(pac, tmp_path):
+    import gzip
+    balls, _, _, _ = golden("1grm_ld_alpha1")
+    crd = tmp_path / "1grm.crd"
+    with open(crd, "w") as f:
+        f.write("%d\n" % len(balls))
+        for b in balls:
+            f.write("%s %s %s %s\n" % tuple(repr(float(v)) for v in b))
+    out = tmp_path / "out.txt"
+    exe = os.path.join(pac.BIN_DIR, "parallelac-largeData")
+    r = subprocess.run([exe, str(crd), str(out), "0", "1", "100000"], capture_output=True,
+                       text=True, env=dict(os.environ, PAC_TET_MODE="as-run"))
+    assert r.returncode == 0, r.stderr
+    assert "Number of tetrahedra:           183" in r.stdout
+    assert out.read_bytes() == gzip.open(os.path.join(GOLDEN, "1grm_ld_alpha1.txt.gz")).read()
+    r = subprocess.run([exe, str(crd)], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stdout.startswith("Usage : parallelac-largeData")
+
+
+# ------------------------------------------------------------ FMA flavour
+def test_fma_flavour_runs_and_is_close(pac, orc):
+    """The contraction-enabled flavour follows the reference binary's default
+    build; against the strict flavour it may differ only on near ties."""
+    balls = pac.globule(3000, seed=21)
+    with _engine(pac, 0, "as-written", "strict") as a, _engine(pac, 0, "as-written", "fma") as b:
+        ra, rb = a.alpha_complex(balls, 1.4, 1.0), b.alpha_complex(balls, 1.4, 1.0)
+    for x, y in ((ra.edges, rb.edges), (ra.tris, rb.tris), (ra.tets, rb.tets)):
+        sx, sy = set(map(tuple, canonical(x))), set(map(tuple, canonical(y)))
+        assert len(sx ^ sy) <= max(5, len(sx) // 1000)

@@ -1,0 +1,210 @@
+"""CPU tests: the restatement (oracle) pinned against the reference's shipped
+outputs and against the reference's own predicates compiled for the host;
+host-side parts of the library (CRD reader, writer, generators, ABI)."""
+import ctypes
+import gzip
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, canonical, golden
+
+
+# ------------------------------------------------------------------ goldens
+def test_oracle_1grm_largedata_golden(orc):
+    """output_files/1grm_pAC_LD_alpha1.txt: upstream formulas, alpha 1, sol 0,
+    produced by a binary whose checkTetsOrthosphere launch fails -> as-run."""
+    balls, E, T, Q = golden("1grm_ld_alpha1")
+    e, t, q, st = orc.alpha_complex(balls, 0.0, 1.0, orc.UPSTREAM, tet_ortho=False)
+    assert (len(e), len(t), len(q)) == (842, 724, 183)
+    np.testing.assert_array_equal(e, E)
+    np.testing.assert_array_equal(t, T)
+    np.testing.assert_array_equal(q, Q)
+
+
+def test_oracle_1grm_plain_golden(orc):
+    """output_files/1grm_pAC_alpha1.txt: plain-xmp formulas (b3 precedence as
+    written at AlphaComplexParallel.cu:344), alpha 1, sol 0."""
+    balls, E, T, Q = golden("1grm_plain_alpha1")
+    e, t, q, _ = orc.alpha_complex(balls, 0.0, 1.0, orc.PLAIN_XMP, tet_ortho=False)
+    np.testing.assert_array_equal(e, E)
+    np.testing.assert_array_equal(t, T)
+    np.testing.assert_array_equal(q, Q)
+
+
+def test_oracle_1k4c_plain_golden_residual(orc):
+    """output_files/1k4c_pAC_alpha1.txt was produced by a binary built with
+    nvcc's default FMA contraction; the restatement has none.  The two agree
+    on all but a few near-tie edge/triangle decisions: this pins the size of
+    that residual (9 edges, 2 triangles of 24737 / 293; tetrahedra identical)."""
+    balls, E, T, Q = golden("1k4c_plain_alpha1")
+    e, t, q, _ = orc.alpha_complex(balls, 0.0, 1.0, orc.PLAIN_XMP, tet_ortho=False)
+    se, sE = set(map(tuple, canonical(e))), set(map(tuple, canonical(E)))
+    st, sT = set(map(tuple, canonical(t))), set(map(tuple, canonical(T)))
+    assert len(se ^ sE) == 9
+    assert len(st ^ sT) == 2
+    np.testing.assert_array_equal(canonical(q), canonical(Q))
+
+
+def test_as_written_differs_from_as_run(orc):
+    """With the orthosphere test applied, the 1grm complex is a proper alpha
+    complex: fewer tetrahedra, and every remaining one is empty."""
+    balls, E, T, Q = golden("1grm_ld_alpha1")
+    e, t, q, st = orc.alpha_complex(balls, 0.0, 1.0, orc.UPSTREAM, tet_ortho=True)
+    assert len(q) < len(Q)
+    assert st["alpha_tets"] == 183 and st["insphere_evals"] > 0
+
+
+# ------------------------------------------------------------------ predicates
+def _predref():
+    from conftest import ge
+    o = ge.load_oracle()
+    if not os.path.exists(o.REF_PRED_PATH):
+        pytest.skip("reference predicates not built here (no reference tree)")
+    L = ctypes.CDLL(o.REF_PRED_PATH)
+    f = ctypes.POINTER(ctypes.c_float)
+    L.ref_exactinit()
+    L.ref_orient3d.restype = ctypes.c_float
+    L.ref_orient3d.argtypes = [f] * 4
+    L.ref_insphere_w.restype = ctypes.c_float
+    L.ref_insphere_w.argtypes = [f] * 5 + [ctypes.c_float] * 5
+    L.ref_sos4.restype = ctypes.c_float
+    L.ref_sos4.argtypes = [f] * 5 + [ctypes.c_float] * 5 + [ctypes.c_int] * 5
+    return L
+
+
+def _p(a):
+    a = np.ascontiguousarray(a, np.float32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def test_insphere_orient_match_reference(orc):
+    """Single-precision orient3d / insphere_w of the restatement equal the
+    reference's predicates.h bit for bit (random inputs, molecular scale)."""
+    L = _predref()
+    rng = np.random.default_rng(7)
+    for _ in range(3000):
+        P = (rng.normal(size=(5, 3)) * 3 + 40).astype(np.float32)
+        W = (rng.uniform(1.4, 3.3, 5) ** 2).astype(np.float32)
+        keep = [_p(x) for x in P]
+        ptr = [k[1] for k in keep]
+        a = L.ref_insphere_w(*ptr, *map(float, W))
+        b = orc.insphere_w(*P, *map(float, W))
+        assert np.float32(a).tobytes() == np.float32(b).tobytes()
+        a = L.ref_orient3d(*ptr[:4])
+        b = orc.orient3d(*P[:4])
+        assert np.float32(a).tobytes() == np.float32(b).tobytes()
+
+
+def test_sos_matches_reference_on_degenerate_sets(orc):
+    """Simulation of simplicity: on lattice points where many minors vanish,
+    the restatement's exact integer SoS gives the reference's sign."""
+    L = _predref()
+    rng = np.random.default_rng(11)
+    depths = set()
+    n = 0
+    while n < 2500:
+        P = (rng.integers(-2, 3, size=(5, 3)) * 0.25 + rng.integers(0, 2) * 17.5).astype(np.float32)
+        W = np.float32(rng.choice([1.5, 1.55, 1.7, 3.1], 5)) ** 2
+        W = W.astype(np.float32)
+        if len({tuple(p) + (w,) for p, w in zip(P.tolist(), W.tolist())}) < 5:
+            continue  # equal weighted points: the reference's SoS never ends
+        idx = rng.permutation(np.arange(1, 6)) * int(rng.integers(1, 1000))
+        keep = [_p(x) for x in P]
+        a = L.ref_sos4(*[k[1] for k in keep], *map(float, W), *map(int, idx))
+        s, d = orc.sos4(P, W, idx)
+        assert d != -1
+        assert np.sign(a) == s, (P, W, idx, a, s, d)
+        depths.add(d)
+        n += 1
+    assert len(depths) >= 4  # several SoS depths were exercised
+
+
+# ------------------------------------------------------------------ ABI, I/O
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "pac.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^[a-z_ ]+\**\s*\**(pac_[a-z0-9_]+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol(pac):
+    names = _declared_functions()
+    assert "pac_alpha_complex" in names and len(names) >= 12
+    L = pac.lib()
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_no_device_fails_loudly(pac):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a device is present")
+    except Exception:
+        pass
+    with pytest.raises(pac.PacError) as ei:
+        pac.Engine()
+    assert ei.value.status == -5
+
+
+def test_crd_reader_matches_reference_parse(pac, tmp_path):
+    balls, _, _, _ = golden("1grm_ld_alpha1")
+    p = tmp_path / "x.crd"
+    with open(p, "w") as f:
+        f.write("%d\n\n" % len(balls))
+        for b in balls:
+            f.write("%s \t%s \t%s \t%s\n" % tuple(repr(float(v)) for v in b))
+    got = pac.read_crd(str(p))
+    assert got.tobytes() == balls.tobytes()
+
+
+def test_crd_reader_errors(pac, tmp_path):
+    p = tmp_path / "bad.crd"
+    p.write_text("3\n1.0 2.0 3.0 1.5\n1.0 2.0\n")
+    with pytest.raises(pac.PacError) as ei:
+        pac.read_crd(str(p))
+    assert ei.value.status == -8
+    with pytest.raises(pac.PacError):
+        pac.read_crd(str(tmp_path / "missing.crd"))
+    p.write_text("0\n")
+    assert pac.read_crd(str(p)).shape == (0, 4)
+
+
+def test_writer_reproduces_reference_file(pac, tmp_path):
+    """The writer emits the golden 1grm output file byte for byte."""
+    balls, E, T, Q = golden("1grm_ld_alpha1")
+
+    class R:
+        edges, tris, tets = E, T, Q
+    out = tmp_path / "o.txt"
+    pac.write_complex(str(out), balls, 0.0, R)
+    want = gzip.open(os.path.join(GOLDEN, "1grm_ld_alpha1.txt.gz")).read()
+    assert out.read_bytes() == want
+
+
+# ------------------------------------------------------------------ generators
+def test_generator_is_deterministic_and_self_avoiding(pac):
+    a = pac.globule(3000, seed=123)
+    b = pac.globule(3000, seed=123)
+    c = pac.globule(3000, seed=124)
+    assert a.tobytes() == b.tobytes() and a.tobytes() != c.tobytes()
+    from scipy.spatial import cKDTree
+    d, _ = cKDTree(a[:, :3].astype(np.float64)).query(a[:, :3].astype(np.float64), k=2)
+    assert d[:, 1].min() >= 1.2 - 1e-4
+    R = (3 * 3000 / (4 * np.pi * 0.05)) ** (1 / 3)
+    assert np.linalg.norm(a[:, :3], axis=1).max() <= R + 1e-3
+    assert set(np.unique(a[:, 3]).tolist()) <= {np.float32(v) for v in (1.70, 1.55, 1.52, 1.80)}
+
+
+def test_snapped_generator_lattice(pac):
+    a = pac.snapped_globule(2000, seed=5)
+    assert np.all(np.abs(a[:, :3] * 4 - np.round(a[:, :3] * 4)) == 0)
+    assert set(np.unique(a[:, 3]).tolist()) <= {np.float32(v) for v in (1.70, 1.55, 1.50, 1.80)}
+
+
+def test_batch_sizes_log_uniform(pac):
+    s = pac.batch_sizes(4096)
+    assert s.min() >= 200 and s.max() <= 20000
+    assert 3500 < s.mean() < 5200
