@@ -193,6 +193,30 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls,
                             float sol_rad, float alpha, pac_batch_complex *out,
                             pac_stats *stats);
 
+/* Union-of-balls volume and surface area over a fixed complex by
+   inclusion-exclusion, with their gradients by a hand-written adjoint.  No
+   reference counterpart: the reference computes only the complex.
+   xyzr: n x 4 doubles (x, y, z, R) with R the grown radius sqrt(r^2 + alpha)
+   of each ball (r including the solvent radius), in input order.  cx: the
+   complex of those balls (host lists, or device lists when cx->on_device ==
+   1).  vol/area: totals.  dvol/darea: n x 4 doubles (d/dx, d/dy, d/dz,
+   d/dR) each, or NULL.  With the weighted alpha complex of the balls at
+   alpha (the dual complex of the grown balls) the totals are the exact
+   volume and area of the union; in every case they are the inclusion-
+   exclusion sums over cx and the gradients are their exact derivatives with
+   cx held fixed.  Gradient sums use floating-point atomics: run-to-run
+   differences are at rounding level. */
+int pac_union_measure(pac_ctx *ctx, const double *xyzr, uint32_t n,
+                      const pac_complex *cx, double *vol, double *area,
+                      double *dvol, double *darea);
+
+/* Same with device-resident inputs and gradient outputs (d_xyzr, d_dvol,
+   d_darea are device pointers; cx must hold device lists, e.g. from
+   pac_alpha_complex_device).  vol/area are host pointers. */
+int pac_union_measure_device(pac_ctx *ctx, const double *d_xyzr, uint32_t n,
+                             const pac_complex *cx, double *vol, double *area,
+                             double *d_dvol, double *d_darea);
+
 void pac_free_complex(pac_complex *cx);
 void pac_free_batch_complex(pac_batch_complex *cx);
 

@@ -69,6 +69,14 @@ int orc_sos4(const float *p0, const float *p1, const float *p2,
              float w3, float w4, int i0, int i1, int i2, int i3, int i4,
              int *depth);
 
+/* FP64 union-of-balls volume and area over a fixed complex by
+   inclusion-exclusion, gradients by forward-mode automatic differentiation
+   (union_oracle.cpp).  xyzr: n x 4 (x, y, z, radius); dvol/darea: n x 4. */
+int orc_union_measure(const double *xyzr, uint32_t n, const uint32_t *edges,
+                      uint64_t ne, const uint32_t *tris, uint64_t nt,
+                      const uint32_t *tets, uint64_t nq, double *vol,
+                      double *area, double *dvol, double *darea);
+
 #ifdef __cplusplus
 }
 #endif

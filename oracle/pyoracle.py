@@ -116,3 +116,36 @@ def canonical(a):
     if len(a) == 0:
         return a
     return a[np.lexsort(a.T[::-1])]
+
+
+def union_measure(xyzr, edges, tris, tets, grad=True):
+    """FP64 union volume/area over the given complex (inclusion-exclusion),
+    gradients by forward-mode AD.  xyzr: (n, 4) float64 with radii already
+    grown (sqrt(r^2 + alpha)).  Returns vol, area, dvol (n,4), darea (n,4)."""
+    L = lib()
+    x = np.ascontiguousarray(xyzr, dtype=np.float64)
+    E = np.ascontiguousarray(edges, dtype=np.uint32)
+    T = np.ascontiguousarray(tris, dtype=np.uint32)
+    Q = np.ascontiguousarray(tets, dtype=np.uint32)
+    n = len(x)
+    vol, area = ctypes.c_double(), ctypes.c_double()
+    dv = np.zeros((n, 4)) if grad else None
+    da = np.zeros((n, 4)) if grad else None
+    P = ctypes.c_void_p
+    L.orc_union_measure.argtypes = [P, ctypes.c_uint32, P, ctypes.c_uint64, P, ctypes.c_uint64, P,
+                                    ctypes.c_uint64, P, P, P, P]
+    L.orc_union_measure(x.ctypes.data, n, E.ctypes.data, len(E), T.ctypes.data, len(T),
+                        Q.ctypes.data, len(Q), ctypes.addressof(vol), ctypes.addressof(area),
+                        dv.ctypes.data if grad else None, da.ctypes.data if grad else None)
+    return vol.value, area.value, dv, da
+
+
+def grown_balls(balls, sol_rad, alpha):
+    """(n, 4) float64: centres and radii sqrt((r + sol)^2 + alpha), with the
+    radius sum in single precision as the complex sees it."""
+    b = np.asarray(balls, dtype=np.float32)
+    r = (b[:, 3] + np.float32(sol_rad)).astype(np.float64)
+    out = np.empty((len(b), 4))
+    out[:, :3] = b[:, :3]
+    out[:, 3] = np.sqrt(r * r + float(alpha))
+    return out

@@ -110,6 +110,8 @@ def _lib():
                                               ctypes.POINTER(Stats)]
         L.pac_cuda_stream.restype = ctypes.c_void_p
         L.pac_cuda_stream.argtypes = [P]
+        L.pac_union_measure.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(Complex), P, P, P, P]
+        L.pac_union_measure_device.argtypes = L.pac_union_measure.argtypes
         L.pac_free_complex.argtypes = [ctypes.POINTER(Complex)]
         L.pac_free_batch_complex.argtypes = [ctypes.POINTER(BatchComplex)]
         L.pac_read_crd.argtypes = [ctypes.c_char_p, ctypes.POINTER(P),
@@ -210,6 +212,11 @@ class Engine:
                                                ctypes.byref(st)))
         return cx, st.as_dict()
 
+    def union_measure(self, xyzr, result, grad=True):
+        """Union volume and area of the balls xyzr ((n, 4) float64, grown
+        radii) over the complex `result`, and their gradients (n, 4)."""
+        return _union(self, xyzr, result, grad)
+
     def alpha_complex_batch(self, balls, offsets, sol_rad, alpha):
         """Many molecules back to back; offsets has n_mol + 1 entries.
         Returns a list of Result (molecule-local indices) and the stats."""
@@ -233,6 +240,38 @@ class Engine:
             return res, st.as_dict()
         finally:
             _lib().pac_free_batch_complex(ctypes.byref(bc))
+
+
+def grown_radii(balls, sol_rad, alpha):
+    """(n, 4) float64 balls for the union measure: centres and radii
+    sqrt((r + sol)^2 + alpha), the radius sum taken in single precision as
+    the complex sees it."""
+    b = np.asarray(balls, dtype=np.float32)
+    r = (b[:, 3] + np.float32(sol_rad)).astype(np.float64)
+    out = np.empty((len(b), 4))
+    out[:, :3] = b[:, :3]
+    out[:, 3] = np.sqrt(r * r + float(alpha))
+    return out
+
+
+def _union(eng, xyzr, result, grad):
+    x = np.ascontiguousarray(xyzr, dtype=np.float64)
+    n = len(x)
+    E = np.ascontiguousarray(result.edges, dtype=np.uint32)
+    T = np.ascontiguousarray(result.tris, dtype=np.uint32)
+    Q = np.ascontiguousarray(result.tets, dtype=np.uint32)
+    cx = Complex(n, 0, len(E), len(T), len(Q),
+                 E.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                 T.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                 Q.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    vol, area = ctypes.c_double(), ctypes.c_double()
+    dv = np.zeros((n, 4)) if grad else None
+    da = np.zeros((n, 4)) if grad else None
+    _check(_lib().pac_union_measure(eng._ctx, x.ctypes.data, n, ctypes.byref(cx),
+                                    ctypes.addressof(vol), ctypes.addressof(area),
+                                    dv.ctypes.data if grad else None,
+                                    da.ctypes.data if grad else None))
+    return vol.value, area.value, dv, da
 
 
 def read_crd(path):

@@ -66,13 +66,16 @@ def build(verbose=False, ptxas_info=False):
          [NVCC] + NVFLAGS + extra + ["-fmad=true", "-DPAC_NS=pac_fma", "-c",
                                      os.path.join(SRC, "pipeline.cu")],
          [os.path.join(SRC, "pipeline.cu")] + hdrs),
+        (os.path.join(OBJ, "union_measure.o"),
+         [NVCC] + NVFLAGS + extra + ["-c", os.path.join(SRC, "union_measure.cu")],
+         [os.path.join(SRC, "union_measure.cu")] + hdrs),
         (os.path.join(OBJ, "engine.o"),
          [NVCC] + NVFLAGS + extra + ["-c", os.path.join(SRC, "engine.cu")],
          [os.path.join(SRC, "engine.cu")] + hdrs),
     ]
     todo = [(o, c + ["-o", o]) for o, c, deps in jobs if _stale(o, deps)]
     logs = []
-    with ThreadPoolExecutor(max_workers=3) as ex:
+    with ThreadPoolExecutor(max_workers=4) as ex:
         for out in ex.map(lambda oc: _run(oc[1]), todo):
             logs.append(out)
     objs = [o for o, _, _ in jobs]

@@ -427,6 +427,63 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
     return PAC_OK;
 }
 
+int pac_union_measure(pac_ctx *ctx, const double *xyzr, uint32_t n, const pac_complex *cx,
+                      double *vol, double *area, double *dvol, double *darea) {
+    if (!ctx || !cx || (n && !xyzr)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    if (cx->n_vertices && cx->n_vertices != n)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "complex and balls differ in size");
+    pac::Ctx &c = ctx->c;
+    cudaSetDevice(c.device);
+    // no arena reset: a device complex from the previous call may live there
+    double4 *d = c.arena.alloc_n<double4>(n);
+    if (!d) return PAC_ERR_OOM;
+    cudaMemcpyAsync(d, xyzr, sizeof(double4) * n, cudaMemcpyHostToDevice, c.stream);
+    const uint32_t *l[3] = {cx->edges, cx->tris, cx->tets};
+    uint64_t cnt[3] = {cx->n_edges, cx->n_tris, cx->n_tets};
+    const uint32_t *dl[3];
+    for (int k = 0; k < 3; k++) {
+        if (cx->on_device == 1 || !cnt[k]) {
+            dl[k] = l[k];
+            continue;
+        }
+        uint32_t *p = c.arena.alloc_n<uint32_t>((k + 2) * cnt[k]);
+        if (!p) return PAC_ERR_OOM;
+        cudaMemcpyAsync(p, l[k], sizeof(uint32_t) * (k + 2) * cnt[k], cudaMemcpyHostToDevice,
+                        c.stream);
+        dl[k] = p;
+    }
+    double *dV = nullptr, *dA = nullptr;
+    if (dvol) dV = c.arena.alloc_n<double>(4 * (size_t)n);
+    if (darea) dA = c.arena.alloc_n<double>(4 * (size_t)n);
+    if ((dvol && !dV) || (darea && !dA)) return PAC_ERR_OOM;
+    if ((dvol && !darea) || (darea && !dvol)) {
+        // the kernel fills both when either is wanted
+        if (!dV) dV = c.arena.alloc_n<double>(4 * (size_t)n);
+        if (!dA) dA = c.arena.alloc_n<double>(4 * (size_t)n);
+    }
+    int rc = pac::union_measure_device(c, d, n, dl[0], cnt[0], dl[1], cnt[1], dl[2], cnt[2], vol,
+                                       area, dV, dA, nullptr);
+    if (rc) return rc;
+    if (dvol) cudaMemcpyAsync(dvol, dV, 4 * sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream);
+    if (darea) cudaMemcpyAsync(darea, dA, 4 * sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream);
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("union measure: ") + cudaGetErrorString(e));
+    return PAC_OK;
+}
+
+int pac_union_measure_device(pac_ctx *ctx, const double *d_xyzr, uint32_t n, const pac_complex *cx,
+                             double *vol, double *area, double *d_dvol, double *d_darea) {
+    if (!ctx || !cx || (n && !d_xyzr)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    if (cx->on_device != 1)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "pac_union_measure_device needs device lists");
+    pac::Ctx &c = ctx->c;
+    cudaSetDevice(c.device);
+    return pac::union_measure_device(c, reinterpret_cast<const double4 *>(d_xyzr), n, cx->edges,
+                                     cx->n_edges, cx->tris, cx->n_tris, cx->tets, cx->n_tets, vol,
+                                     area, d_dvol, d_darea, nullptr);
+}
+
 void pac_free_complex(pac_complex *cx) {
     if (!cx) return;
     if (cx->on_device == 2) {

@@ -68,6 +68,11 @@ struct Ctx {
     int launches = 0;
 };
 
+int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uint32_t *d_edges,
+                         uint64_t ne, const uint32_t *d_tris, uint64_t nt, const uint32_t *d_tets,
+                         uint64_t nq, double *vol, double *area, double *d_dV, double *d_dA,
+                         float *ms);
+
 // Sets the thread-local error detail; returns status.
 int set_error(int status, const std::string &msg);
 

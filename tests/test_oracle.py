@@ -208,3 +208,44 @@ def test_batch_sizes_log_uniform(pac):
     s = pac.batch_sizes(4096)
     assert s.min() >= 200 and s.max() <= 20000
     assert 3500 < s.mean() < 5200
+
+
+# ------------------------------------------------------------------ reference runs
+def _refrun_manifest():
+    import json
+    return json.load(open(os.path.join(GOLDEN, "refrun", "refrun_manifest.json")))
+
+
+def _refrun_inputs(pac):
+    return {"1grm_a1": (golden("1grm_ld_alpha1")[0], 0.0, 1.0),
+            "1k4c_a1": (golden("1k4c_plain_alpha1")[0], 0.0, 1.0),
+            "glob1300_a0": (pac.globule(1300, seed=pac.SEED_BASE), 0.0, 0.0),
+            "glob5000_s14_a1": (pac.globule(5000, seed=pac.SEED_BASE + 4), 1.4, 1.0)}
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint32).tobytes()).hexdigest()
+
+
+def test_oracle_matches_reference_binary_runs(pac, orc):
+    """The reference's own AlphaComplexLargeData.cu, built with -fmad=false
+    and -maxrregcount=128 (so that checkTetsOrthosphere launches) and run on
+    a B200 (tests/golden/make_refrun_golden.py), gave these lists: the
+    restatement reproduces them bit for bit, in order."""
+    man = _refrun_manifest()
+    for name, (balls, sol, alpha) in _refrun_inputs(pac).items():
+        rec = man[name]["builds"]["rr128-nofma"]
+        e, t, q, _ = orc.alpha_complex(balls, sol, alpha, orc.UPSTREAM, tet_ortho=True)
+        assert [_sha(e), _sha(t), _sha(q)] == rec["sha256"], name
+
+
+def test_default_reference_build_aborts_on_b200():
+    """Built with default flags, the reference aborts on a B200 once
+    checkTetsOrthosphere fails to launch; recorded, not re-run."""
+    man = _refrun_manifest()
+    for name, e in man.items():
+        if "skipped" in e:
+            continue
+        assert e["builds"]["default"]["rc"] != 0
+        assert "system_error" in e["builds"]["default"]["log_tail"]
