@@ -222,6 +222,23 @@ def main():
         barrier()
         wall = time.perf_counter() - t0
     dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # ---- union volume/area and their gradients on the final complex
+    xyzr = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
+    dvol = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    darea = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    cx, _ = eng.alpha_complex_device(d_balls.data_ptr(), n, SOL, ALPHA)
+    for _ in range(2):
+        eng.union_measure_device(xyzr.data_ptr(), n, cx, dvol.data_ptr(), darea.data_ptr())
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for k in range(args.steps):
+        gev[k][0].record(stream)
+        uvol, uarea = eng.union_measure_device(xyzr.data_ptr(), n, cx, dvol.data_ptr(),
+                                               darea.data_ptr())
+        gev[k][1].record(stream)
+    torch.cuda.synchronize()
+    grad_ms = sum(a.elapsed_time(b) for a, b in gev) / args.steps
     t_max = dev_ms
     if dist:
         t = torch.tensor([dev_ms], device="cuda")
@@ -286,6 +303,8 @@ def main():
                     "insphere_evals": s0["insphere_evals"], "sos_calls": s0["sos_calls"]},
         "stage_ms": {k: s0[k] for k in ("ms_grid", "ms_edges", "ms_tris", "ms_tets",
                                         "ms_tri_attach", "ms_edge_attach", "ms_emit")},
+        "union": {"grad_ms": grad_ms, "volume": uvol, "area": uarea,
+                  "what": "volume + area + d/d(centre, radius) of both, FP64, over the final complex"},
         "e2e": {"value": e2e_value, "unit": "balls/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -107,9 +107,13 @@ typedef struct {
     float x, y, z, r;
 } pac_ball;
 
-/* One complex.  Lists are owned by the library and released with
-   pac_free_complex().  on_device = 1 means the three pointers are device
-   pointers (from pac_alpha_complex_device). */
+/* One complex.  on_device says where the three lists live:
+     0  host memory allocated by the caller (e.g. for pac_write_complex)
+     1  device memory of the context (pac_alpha_complex_device)
+     3  pinned host memory of the context (pac_alpha_complex)
+   Lists of kinds 1 and 3 belong to the context and stay valid until its next
+   call or pac_destroy; copy them to keep them longer.  pac_free_complex()
+   resets the struct (and frees nothing for those kinds). */
 typedef struct {
     uint32_t n_vertices;
     uint32_t on_device;
@@ -120,7 +124,9 @@ typedef struct {
 } pac_complex;
 
 /* Many molecules: the lists of molecule m are rows [off[m], off[m+1]) of
-   the concatenated lists, with molecule-local vertex indices. */
+   the concatenated lists, with molecule-local vertex indices.  The lists are
+   context-owned pinned host memory (on_device = 3, valid until the next call);
+   the offset arrays are malloc'ed and freed by pac_free_batch_complex(). */
 typedef struct {
     uint32_t n_mol;
     uint32_t on_device;

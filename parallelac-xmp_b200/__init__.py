@@ -217,6 +217,17 @@ class Engine:
         radii) over the complex `result`, and their gradients (n, 4)."""
         return _union(self, xyzr, result, grad)
 
+    def union_measure_device(self, d_xyzr_ptr, n, cx, d_dvol_ptr=0, d_darea_ptr=0):
+        """Device variant: d_xyzr_ptr (n x 4 doubles) and the gradient
+        buffers are device pointers; cx a Complex with device lists (from
+        alpha_complex_device).  Returns (vol, area)."""
+        vol, area = ctypes.c_double(), ctypes.c_double()
+        _check(_lib().pac_union_measure_device(
+            self._ctx, ctypes.c_void_p(d_xyzr_ptr), n, ctypes.byref(cx), ctypes.addressof(vol),
+            ctypes.addressof(area), ctypes.c_void_p(d_dvol_ptr or None),
+            ctypes.c_void_p(d_darea_ptr or None)))
+        return vol.value, area.value
+
     def alpha_complex_batch(self, balls, offsets, sol_rad, alpha):
         """Many molecules back to back; offsets has n_mol + 1 entries.
         Returns a list of Result (molecule-local indices) and the stats."""

@@ -136,17 +136,38 @@ int validate_opts(const pac_options &o) {
     return PAC_OK;
 }
 
-template <class T>
-int to_pinned(const T *d, uint64_t count, T **h, cudaStream_t s) {
-    *h = nullptr;
-    if (!count) return PAC_OK;
-    if (cudaMallocHost((void **)h, sizeof(T) * count) != cudaSuccess) {
-        cudaGetLastError();
-        return pac::set_error(PAC_ERR_OOM, "cudaMallocHost for the output lists failed");
+// Copies the three device lists into the context's pinned buffer (grown if
+// needed) and points the outputs at it.
+int lists_to_host(pac::Ctx &c, const pac::PassOutput &po, uint32_t **e, uint32_t **t,
+                  uint32_t **q) {
+    size_t ne = 2 * po.n_edges, nt = 3 * po.n_tris, nq = 4 * po.n_tets;
+    size_t need = sizeof(uint32_t) * (ne + nt + nq);
+    if (need > c.pinned_size) {
+        if (c.pinned) cudaFreeHost(c.pinned);
+        c.pinned = nullptr;
+        c.pinned_size = 0;
+        size_t sz = std::max(need + need / 4, size_t(1) << 20);
+        if (cudaMallocHost(&c.pinned, sz) != cudaSuccess) {
+            cudaGetLastError();
+            return pac::set_error(PAC_ERR_OOM, "cudaMallocHost for the output lists failed");
+        }
+        c.pinned_size = sz;
     }
-    cudaError_t e = cudaMemcpyAsync(*h, d, sizeof(T) * count, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess)
-        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    uint32_t *base = static_cast<uint32_t *>(c.pinned);
+    *e = ne ? base : nullptr;
+    *t = nt ? base + ne : nullptr;
+    *q = nq ? base + ne + nt : nullptr;
+    cudaError_t err = cudaSuccess;
+    if (ne && err == cudaSuccess)
+        err = cudaMemcpyAsync(base, po.d_edges, sizeof(uint32_t) * ne, cudaMemcpyDeviceToHost, c.stream);
+    if (nt && err == cudaSuccess)
+        err = cudaMemcpyAsync(base + ne, po.d_tris, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost,
+                              c.stream);
+    if (nq && err == cudaSuccess)
+        err = cudaMemcpyAsync(base + ne + nt, po.d_tets, sizeof(uint32_t) * nq,
+                              cudaMemcpyDeviceToHost, c.stream);
+    if (err != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(err));
     return PAC_OK;
 }
 
@@ -227,6 +248,7 @@ int pac_destroy(pac_ctx *ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     for (auto &ev : ctx->c.ev)
         if (ev) cudaEventDestroy(ev);
+    if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
     cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return PAC_OK;
@@ -305,10 +327,8 @@ int pac_alpha_complex(pac_ctx *ctx, const pac_ball *balls, uint32_t n, float sol
     out->n_edges = po.n_edges;
     out->n_tris = po.n_tris;
     out->n_tets = po.n_tets;
-    out->on_device = 2;  // pinned host memory
-    if ((rc = to_pinned(po.d_edges, 2 * po.n_edges, &out->edges, c.stream)) ||
-        (rc = to_pinned(po.d_tris, 3 * po.n_tris, &out->tris, c.stream)) ||
-        (rc = to_pinned(po.d_tets, 4 * po.n_tets, &out->tets, c.stream))) {
+    out->on_device = 3;  // context-owned pinned host memory
+    if ((rc = lists_to_host(c, po, &out->edges, &out->tris, &out->tets))) {
         pac_free_complex(out);
         return rc;
     }
@@ -364,7 +384,7 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
             koff.push_back(offsets[m + 1]);
         }
     out->n_mol = n_mol;
-    out->on_device = 2;
+    out->on_device = 3;
     out->edge_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
     out->tri_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
     out->tet_off = (uint64_t *)std::calloc(n_mol + 1, sizeof(uint64_t));
@@ -390,9 +410,8 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
         pac_free_batch_complex(out);
         return rc;
     }
-    if ((rc = to_pinned(po.d_edges, 2 * po.n_edges, &out->edges, c.stream)) ||
-        (rc = to_pinned(po.d_tris, 3 * po.n_tris, &out->tris, c.stream)) ||
-        (rc = to_pinned(po.d_tets, 4 * po.n_tets, &out->tets, c.stream))) {
+    out->on_device = 3;
+    if ((rc = lists_to_host(c, po, &out->edges, &out->tris, &out->tets))) {
         pac_free_batch_complex(out);
         return rc;
     }
@@ -495,18 +514,14 @@ void pac_free_complex(pac_complex *cx) {
         std::free(cx->tris);
         std::free(cx->tets);
     }
-    // on_device == 1: lists live in the context's pool until its next call
+    // on_device == 1 (device pool) or 3 (pinned host buffer): the lists
+    // belong to the context and stay valid until its next call
     cx->edges = cx->tris = cx->tets = nullptr;
     cx->n_edges = cx->n_tris = cx->n_tets = 0;
 }
 
 void pac_free_batch_complex(pac_batch_complex *cx) {
     if (!cx) return;
-    if (cx->on_device == 2) {
-        if (cx->edges) cudaFreeHost(cx->edges);
-        if (cx->tris) cudaFreeHost(cx->tris);
-        if (cx->tets) cudaFreeHost(cx->tets);
-    }
     std::free(cx->edge_off);
     std::free(cx->tri_off);
     std::free(cx->tet_off);

@@ -66,6 +66,10 @@ struct Ctx {
     pac_options opt{};
     cudaEvent_t ev[16]{};
     int launches = 0;
+    // pinned host memory for the lists returned by the host entry points;
+    // grows, never shrinks, reused by every call
+    void *pinned = nullptr;
+    size_t pinned_size = 0;
 };
 
 int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uint32_t *d_edges,

@@ -47,7 +47,7 @@ constexpr unsigned kFull = 0xffffffffu;
 // device-side counters (one slot each)
 enum Counter {
     C_CAND_E, C_ALPHA_E, C_CAND_T, C_ALPHA_T, C_CAND_Q, C_ALPHA_Q, C_INSPHERE, C_SOS,
-    C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NCOUNTERS
+    C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NEXT, C_NCOUNTERS
 };
 
 struct MolGrid {
@@ -729,6 +729,385 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
     }
 }
 
+// As-written tetrahedra, one warp per ball v1, in three balanced phases:
+//  1. the candidate fourth vertices of every alpha triangle (v1, v2, v3) are
+//     flattened over the lanes (bits of rows a and b of v1's link matrix,
+//     checked against v2's link matrix), so each lane tests one candidate;
+//  2. each candidate gets markRealTets' alpha test, and the passing ones are
+//     queued in shared memory with their orthosphere's window cell;
+//  3. the queue is drained by work stealing: every lane owns one queued
+//     tetrahedron at a time and evaluates one window ball per step (the
+//     empty-orthosphere test of checkTetsOrthosphere), taking the next
+//     queued tetrahedron as soon as its own is decided.
+// The result does not depend on the order of the window balls: a
+// tetrahedron survives only if no ball violates its orthosphere.
+constexpr int kQCap = 192;
+
+__device__ __forceinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
+                                              const uint32_t *N, uint32_t key, bool pending,
+                                              uint32_t &ball_count) {
+    if (pending) {
+        unsigned long long q = atomicAdd(&A.ctr[C_PEND], 1ull);
+        if (q < A.pend_cap) A.pend[q] = make_uint2((uint32_t)p, key);
+        return;
+    }
+    unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
+    if (q < A.surv_cap) A.surv[q] = make_uint2((uint32_t)p, key);
+    ball_count++;
+    int a = key & 0xff, b = (key >> 8) & 0xff, c = (key >> 16) & 0xff;
+    mark_face(A.faces, lp, W, a, b);
+    mark_face(A.faces, lp, W, a, c);
+    mark_face(A.faces, lp, W, b, c);
+    const uint32_t v2 = N[a];
+    const uint64_t e2 = A.eoff[v2];
+    const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+    const int mb = lbound(A.ER + e2, deg2, N[b]), mc = lbound(A.ER + e2, deg2, N[c]);
+    mark_face(A.faces, A.loff[v2], (deg2 + 63) >> 6, mb, mc);
+}
+
+constexpr int kLongCap = 32;   // tetrahedra handed to the cooperative scan
+constexpr int kSerialEvals = 8; // window balls a lane scans alone before handing off
+
+// Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
+// lane k < 27 owns window cell k (the centre cell through its linear index,
+// then the 26 neighbours range-checked per axis), a prefix sum over the cell
+// sizes flattens the window balls over the lanes.  Returns 1 = violated,
+// 2 = no violation but an exact zero, 0 = empty.
+__device__ __forceinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
+                                         uint32_t v2, uint32_t v3, uint32_t v4, const float *pa,
+                                         const float *pb, const float *pc, const float *pd,
+                                         float wa, float wb, float wc, float wd,
+                                         float orientation, int4 cl,
+                                         unsigned long long &evals) {
+    const int lane = threadIdx.x & 31;
+    uint32_t beg = 0, cnt = 0;
+    if (lane == 0) {
+        if (cl.w >= 0 && (uint64_t)cl.w < G.ncell) {
+            uint64_t gc = G.cell_base + (uint64_t)cl.w;
+            beg = A.cellbeg[gc];
+            cnt = A.cellbeg[gc + 1] - beg;
+        }
+    } else if (lane < 27) {
+        int rr = lane - 1 + (lane >= 14 ? 1 : 0);
+        int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
+        int zz = (int)((unsigned)cl.z + (unsigned)i), yy = (int)((unsigned)cl.y + (unsigned)j),
+            xx = (int)((unsigned)cl.x + (unsigned)k);
+        if (!((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) && !((zz < 0) || (yy < 0) || (xx < 0))) {
+            uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+            beg = A.cellbeg[gc];
+            cnt = A.cellbeg[gc + 1] - beg;
+        }
+    }
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    bool zero = false;
+    for (uint32_t base = 0; base < total; base += 32) {
+        uint32_t s = base + lane;
+        int lo = 0;
+        for (int step = 16; step; step >>= 1) {
+            uint32_t v = __shfl_sync(kFull, incl, lo + step - 1);
+            if (v <= s) lo += step;
+        }
+        const uint32_t sinc = __shfl_sync(kFull, incl, lo & 31);
+        const uint32_t sbeg = __shfl_sync(kFull, beg, lo & 31);
+        const uint32_t scnt = __shfl_sync(kFull, cnt, lo & 31);
+        bool viol = false;
+        if (s < total) {
+            uint32_t x = sbeg + (s - (sinc - scnt));
+            if (!(x == v1 || x == v2 || x == v3 || x == v4)) {
+                const Ball atom = pac::ld_ball(&A.at[x]);
+                float pe[3];
+                pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
+                float we = atom.r * atom.r;
+                evals++;
+                float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+                viol = orientation < 0 ? (result < 0) : (result > 0);
+                if (result == 0) zero = true;
+            }
+        }
+        if (__any_sync(kFull, viol)) return 1;
+    }
+    return __any_sync(kFull, zero) ? 2 : 0;
+}
+
+template <int V>
+__global__ void __launch_bounds__(256, 2) k_tets_ws(TetArgs A) {
+    __shared__ uint16_t smap[8][kMaxDeg];
+    __shared__ uint32_t qkey[8][kQCap];
+    __shared__ int4 qcell[8][kQCap];
+    __shared__ uint32_t lkey[8][kLongCap];
+    __shared__ int4 lcell[8][kLongCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1;
+    unsigned long long cand_acc = 0, alpha_acc = 0, evals = 0, oob = 0;
+    while (true) {
+        uint64_t p = 0;
+        if (lane == 0) p = atomicAdd(&A.ctr[C_NEXT], 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= A.n) break;
+        const uint64_t e0 = A.eoff[p];
+        const int deg = (int)(A.eoff[p + 1] - e0);
+        uint32_t ball_count = 0;
+        if (deg >= 3) {
+            const int W = (deg + 63) >> 6;
+            const uint32_t *N = A.ER + e0;
+            const uint64_t lp = A.loff[p];
+            const uint64_t *Lp = A.link + lp;
+            const Ball B1 = pac::ld_ball(&A.at[p]);
+            const MolGrid G = A.grids[mol_of(A.mol, p)];
+            int qn = 0;
+
+            // phase 3: drain the queue (work stealing across the lanes)
+            auto drain = [&]() {
+                int head = 0;
+                bool have = false;
+                uint32_t key = 0;
+                float pa[3], pb[3], pc[3], pd[3], wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
+                uint32_t v2 = 0, v3 = 0, v4 = 0;
+                int gX = 0, gY = 0, gZ = 0, q = 0, nev = 0;
+                int4 mycell = make_int4(0, 0, 0, 0);
+                uint32_t e = 0, end = 0;
+                bool zero = false;
+                int ln = 0;  // long queue length (warp-uniform)
+                while (true) {
+                    unsigned want = __ballot_sync(kFull, !have);
+                    if (want && head < qn) {
+                        int r = __popc(want & lt_mask);
+                        if (!have && head + r < qn) {
+                            int idx = head + r;
+                            key = qkey[wib][idx];
+                            int4 cl = qcell[wib][idx];
+                            v2 = __ldg(&N[key & 0xff]);
+                            v3 = __ldg(&N[(key >> 8) & 0xff]);
+                            v4 = __ldg(&N[(key >> 16) & 0xff]);
+                            const Ball a2 = pac::ld_ball(&A.at[v2]), a3 = pac::ld_ball(&A.at[v3]),
+                                       a4 = pac::ld_ball(&A.at[v4]);
+                            pa[0] = B1.x, pa[1] = B1.y, pa[2] = B1.z, wa = B1.r * B1.r;
+                            pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
+                            pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
+                            pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
+                            orientation = pac::orient3d(pa, pb, pc, pd);
+                            gX = cl.x;
+                            gY = cl.y;
+                            gZ = cl.z;
+                            mycell = cl;
+                            int cc = cl.w;
+                            q = 0;
+                            nev = 0;
+                            zero = false;
+                            if (cc >= 0 && (uint64_t)cc < G.ncell) {
+                                uint64_t gc = G.cell_base + (uint64_t)cc;
+                                e = A.cellbeg[gc];
+                                end = A.cellbeg[gc + 1];
+                            } else {
+                                e = end = 0;
+                                oob++;
+                            }
+                            have = true;
+                        }
+                        head = min(qn, head + __popc(want));
+                    }
+                    if (!__any_sync(kFull, have)) break;
+                    // a tetrahedron still open after kSerialEvals balls goes to
+                    // the cooperative scan, so no lane runs a long window alone
+                    const bool handoff = have && nev >= kSerialEvals;
+                    const unsigned hm = __ballot_sync(kFull, handoff);
+                    if (hm) {
+                        int pos = ln + __popc(hm & lt_mask);
+                        if (handoff && pos < kLongCap) {
+                            lkey[wib][pos] = key;
+                            lcell[wib][pos] = mycell;
+                            have = false;
+                        }
+                        ln = min(kLongCap, ln + __popc(hm));
+                    }
+                    if (!have) continue;
+                    if (e < end) {
+                        uint32_t x = e++;
+                        if (x == (uint32_t)p || x == v2 || x == v3 || x == v4) continue;
+                        const Ball atom = pac::ld_ball(&A.at[x]);
+                        float pe[3];
+                        pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
+                        float we = atom.r * atom.r;
+                        evals++;
+                        nev++;
+                        float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+                        bool viol = orientation < 0 ? (result < 0) : (result > 0);
+                        if (viol) {
+                            have = false;
+                            continue;
+                        }
+                        if (result == 0) zero = true;
+                        continue;
+                    }
+                    // next window cell: the 26 neighbours of the centre cell,
+                    // range-checked per axis (AlphaComplexLargeData.cu:673-685)
+                    bool found = false;
+                    while (q < 26 && !found) {
+                        q++;
+                        int rr = q - 1 + (q >= 14 ? 1 : 0);
+                        int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
+                        int zz = (int)((unsigned)gZ + (unsigned)i),
+                            yy = (int)((unsigned)gY + (unsigned)j),
+                            xx = (int)((unsigned)gX + (unsigned)k);
+                        if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
+                        if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+                        uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
+                        e = A.cellbeg[gc];
+                        end = A.cellbeg[gc + 1];
+                        found = true;
+                    }
+                    if (!found) {
+                        emit_survivor(A, p, W, lp, N, key, zero, ball_count);
+                        have = false;
+                    }
+                }
+                __syncwarp();
+                for (int t = 0; t < ln; t++) {
+                    const uint32_t k2 = lkey[wib][t];
+                    const int4 cl = lcell[wib][t];
+                    const uint32_t u2 = __ldg(&N[k2 & 0xff]), u3 = __ldg(&N[(k2 >> 8) & 0xff]),
+                                   u4 = __ldg(&N[(k2 >> 16) & 0xff]);
+                    const Ball a2 = pac::ld_ball(&A.at[u2]), a3 = pac::ld_ball(&A.at[u3]),
+                               a4 = pac::ld_ball(&A.at[u4]);
+                    float qa[3], qb[3], qc[3], qd[3];
+                    qa[0] = B1.x, qa[1] = B1.y, qa[2] = B1.z;
+                    qb[0] = a2.x, qb[1] = a2.y, qb[2] = a2.z;
+                    qc[0] = a3.x, qc[1] = a3.y, qc[2] = a3.z;
+                    qd[0] = a4.x, qd[1] = a4.y, qd[2] = a4.z;
+                    const float xa = B1.r * B1.r, xb = a2.r * a2.r, xc = a3.r * a3.r,
+                                xd = a4.r * a4.r;
+                    const float ori = pac::orient3d(qa, qb, qc, qd);
+                    int r = coop_test(A, G, (uint32_t)p, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc,
+                                      xd, ori, cl, evals);
+                    if (r != 1 && lane == 0) emit_survivor(A, p, W, lp, N, k2, r == 2, ball_count);
+                }
+                __syncwarp();
+            };
+
+            for (int a = 0; a < deg - 2; a++) {
+                uint64_t ra[kMaxW];
+                int nb = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
+                    nb += __popcll(ra[w]);
+                }
+                if (nb < 2) continue;
+                const uint32_t v2 = __ldg(&N[a]);
+                const uint64_t e2 = A.eoff[v2];
+                const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+                const int W2 = (deg2 + 63) >> 6;
+                const uint64_t *L2 = A.link + A.loff[v2];
+                for (int c = a + 1 + lane; c < deg; c += 32) {
+                    uint32_t x = __ldg(&N[c]);
+                    int pos = lbound(A.ER + e2, deg2, x);
+                    smap[wib][c] = (pos < deg2 && __ldg(&A.ER[e2 + pos]) == x) ? (uint16_t)pos
+                                                                               : (uint16_t)0xffff;
+                }
+                __syncwarp();
+                const Ball B2 = pac::ld_ball(&A.at[v2]);
+                for (int k0 = 0; k0 < nb; k0 += 32) {
+                    // phase 1: this lane's alpha triangle (v1, v2, N[b]) and its
+                    // candidate fourth vertices
+                    int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
+                    uint64_t m[kMaxW];
+                    int cnt = 0;
+#pragma unroll
+                    for (int w = 0; w < kMaxW; w++) {
+                        m[w] = (b >= 0 && w < W) ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
+                                                 : 0;
+                        cnt += __popcll(m[w]);
+                    }
+                    int incl = cnt;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        int v = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += v;
+                    }
+                    const int total = __shfl_sync(kFull, incl, 31);
+                    for (int base = 0; base < total; base += 32) {
+                        const int s = base + lane;
+                        int lo = 0;
+                        for (int step = 16; step; step >>= 1) {
+                            int v = __shfl_sync(kFull, incl, lo + step - 1);
+                            if (v <= s) lo += step;
+                        }
+                        const int owner = lo & 31;
+                        const int oincl = __shfl_sync(kFull, incl, owner);
+                        const int ocnt = __shfl_sync(kFull, cnt, owner);
+                        const int bo = __shfl_sync(kFull, b, owner);
+                        uint64_t mo[kMaxW];
+#pragma unroll
+                        for (int w = 0; w < kMaxW; w++) {
+                            uint32_t lo32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
+                            uint32_t hi32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
+                            mo[w] = ((uint64_t)hi32 << 32) | lo32;
+                        }
+                        bool pass4 = false, passA = false;
+                        int c = -1;
+                        int4 cell = make_int4(0, 0, 0, 0);
+                        if (s < total) {
+                            c = select_bit(mo, W, s - (oincl - ocnt));
+                            const int mb = smap[wib][bo], mc = smap[wib][c];
+                            pass4 = mb != 0xffff && mc != 0xffff &&
+                                    ((__ldg(&L2[(uint64_t)mb * W2 + (mc >> 6)]) >> (mc & 63)) & 1ull);
+                            if (pass4) {
+                                const Ball B3 = pac::ld_ball(&A.at[__ldg(&N[bo])]);
+                                const Ball B4 = pac::ld_ball(&A.at[__ldg(&N[c])]);
+                                float4 sphere;
+                                passA = pac::tet_alpha(B1, B2, B3, B4, A.alpha, sphere);
+                                if (passA) {
+                                    int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
+                                    int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
+                                    int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
+                                    cell = make_int4(gridX, gridY, gridZ,
+                                                     lin3(gridX, gridY, gridZ, G.gx, G.gy));
+                                }
+                            }
+                        }
+                        const unsigned m4 = __ballot_sync(kFull, pass4);
+                        const unsigned mA = __ballot_sync(kFull, passA);
+                        if (passA) {
+                            int pos = qn + __popc(mA & lt_mask);
+                            qkey[wib][pos] = (uint32_t)a | ((uint32_t)bo << 8) | ((uint32_t)c << 16);
+                            qcell[wib][pos] = cell;
+                        }
+                        qn += __popc(mA);
+                        cand_acc += lane == 0 ? __popc(m4) : 0;
+                        alpha_acc += lane == 0 ? __popc(mA) : 0;
+                        __syncwarp();
+                        if (qn > kQCap - 32) {
+                            drain();
+                            qn = 0;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            if (qn) drain();
+        }
+        {
+            uint32_t s = ball_count;
+            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+            if (lane == 0) A.tcount[p] = s;
+        }
+    }
+    cand_acc = warp_sum(cand_acc);
+    alpha_acc = warp_sum(alpha_acc);
+    evals = warp_sum(evals);
+    oob = warp_sum(oob);
+    if (lane == 0) {
+        bump(A.ctr, C_CAND_Q, cand_acc);
+        bump(A.ctr, C_ALPHA_Q, alpha_acc);
+        bump(A.ctr, C_INSPHERE, evals);
+        bump(A.ctr, C_OOB, oob);
+    }
+}
+
 // Tetrahedra whose window holds an insphere value of exactly 0: the test
 // again, with the reference's simulation of simplicity for those balls
 // (AlphaComplexLargeData.cu:645-652, 659-667).
@@ -1305,7 +1684,8 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
             CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
             CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
-            k_tets<V, 0><<<warp_blocks(n), 256, 0, s>>>(T);
+            CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+            k_tets_ws<V><<<std::min<unsigned>(warp_blocks(n), 148 * 2), 256, 0, s>>>(T);
             LAUNCH_CHECK(ctx);
             unsigned long long sp[2];
             CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(sp), cudaMemcpyDeviceToHost, s));

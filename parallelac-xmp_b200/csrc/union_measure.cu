@@ -218,17 +218,27 @@ __device__ void simplex_terms(int k, const V3 *c, const double *R, Terms &T) {
     T.V = vol / 3.0;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+// double-double accumulation (TwoSum), so the totals do not depend on the
+// order in which the blocks finish: each block reduces its simplices in a
+// fixed shuffle/shared-memory order and writes one (hi, lo) pair; one block
+// then sums the pairs in index order.
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double bh, double bl) {
+    double s = hi + bh;
+    double v = s - hi;
+    double e = (hi - (s - v)) + (bh - v);
+    e += lo + bl;
+    hi = s + e;
+    lo = e - (hi - s);
 }
 
 // one thread per simplex; simplices of dimension dim with k = dim + 1
 // vertices, indices in idx[k * s + ...]
-__global__ void k_union(int k, uint64_t ns, const uint32_t *idx, const double4 *balls,
-                        double *acc /* vol, area */, double *dV, double *dA, int want_grad) {
+__global__ void __launch_bounds__(128) k_union(int k, uint64_t ns, const uint32_t *idx,
+                                               const double4 *balls, double4 *partial,
+                                               double *dV, double *dA, int want_grad) {
+    __shared__ double4 wpart[4];
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0, a = 0;
+    double vh = 0, vl = 0, ah = 0, al = 0;
     if (s < ns) {
         uint32_t id[4];
         V3 c[4];
@@ -244,8 +254,8 @@ __global__ void k_union(int k, uint64_t ns, const uint32_t *idx, const double4 *
         Terms T;
         simplex_terms(k, c, R, T);
         double sg = (k & 1) ? 1.0 : -1.0;
-        v = sg * T.V;
-        for (int q = 0; q < k; q++) a += sg * T.A[q];
+        vh = sg * T.V;
+        for (int q = 0; q < k; q++) dd_add(ah, al, sg * T.A[q], 0.0);
         if (want_grad)
             for (int q = 0; q < k; q++) {
                 double *gv = dV + 4 * (uint64_t)id[q], *ga = dA + 4 * (uint64_t)id[q];
@@ -260,11 +270,42 @@ __global__ void k_union(int k, uint64_t ns, const uint32_t *idx, const double4 *
                 atomicAdd(ga + 3, sg * (inv * T.A[q] + T.rl[q]));
             }
     }
-    v = warp_sum(v);
-    a = warp_sum(a);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&acc[0], v);
-        atomicAdd(&acc[1], a);
+    for (int o = 16; o; o >>= 1) {
+        double h1 = __shfl_xor_sync(0xffffffffu, vh, o), l1 = __shfl_xor_sync(0xffffffffu, vl, o);
+        double h2 = __shfl_xor_sync(0xffffffffu, ah, o), l2 = __shfl_xor_sync(0xffffffffu, al, o);
+        dd_add(vh, vl, h1, l1);
+        dd_add(ah, al, h2, l2);
+    }
+    if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = make_double4(vh, vl, ah, al);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double4 r = wpart[0];
+        for (int w = 1; w < 4; w++) {
+            dd_add(r.x, r.y, wpart[w].x, wpart[w].y);
+            dd_add(r.z, r.w, wpart[w].z, wpart[w].w);
+        }
+        partial[blockIdx.x] = r;
+    }
+}
+
+__global__ void k_union_total(const double4 *partial, uint64_t np, double *out) {
+    __shared__ double4 sp[256];
+    double vh = 0, vl = 0, ah = 0, al = 0;
+    for (uint64_t i = threadIdx.x; i < np; i += 256) {
+        double4 r = partial[i];
+        dd_add(vh, vl, r.x, r.y);
+        dd_add(ah, al, r.z, r.w);
+    }
+    sp[threadIdx.x] = make_double4(vh, vl, ah, al);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double4 r = sp[0];
+        for (int t = 1; t < 256; t++) {
+            dd_add(r.x, r.y, sp[t].x, sp[t].y);
+            dd_add(r.z, r.w, sp[t].z, sp[t].w);
+        }
+        out[0] = r.x + r.y;
+        out[1] = r.z + r.w;
     }
 }
 
@@ -284,25 +325,31 @@ int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uin
     double *dV = d_dV, *dA = d_dA;
     if (grad && !dV) dV = ctx.arena.alloc_n<double>(4 * (size_t)n);
     if (grad && !dA) dA = ctx.arena.alloc_n<double>(4 * (size_t)n);
-    if (!acc || (grad && (!dV || !dA))) return PAC_ERR_OOM;
+    const uint32_t *lists[4] = {nullptr, d_edges, d_tris, d_tets};
+    uint64_t counts[4] = {n, ne, nt, nq};
+    uint64_t nblocks = 0;
+    for (int k = 0; k < 4; k++) nblocks += (counts[k] + 127) / 128;
+    double4 *partial = ctx.arena.alloc_n<double4>(nblocks);
+    if (!acc || !partial || (grad && (!dV || !dA))) return PAC_ERR_OOM;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    cudaMemsetAsync(acc, 0, 2 * sizeof(double), s);
     if (grad) {
         cudaMemsetAsync(dV, 0, 4 * sizeof(double) * n, s);
         cudaMemsetAsync(dA, 0, 4 * sizeof(double) * n, s);
     }
-    const uint32_t *lists[4] = {nullptr, d_edges, d_tris, d_tets};
-    uint64_t counts[4] = {n, ne, nt, nq};
+    uint64_t off = 0;
     for (int k = 1; k <= 4; k++) {
         if (!counts[k - 1]) continue;
         unsigned blocks = (unsigned)((counts[k - 1] + 127) / 128);
-        pac_union::k_union<<<blocks, 128, 0, s>>>(k, counts[k - 1], lists[k - 1], d_balls, acc, dV,
-                                                  dA, grad ? 1 : 0);
+        pac_union::k_union<<<blocks, 128, 0, s>>>(k, counts[k - 1], lists[k - 1], d_balls,
+                                                  partial + off, dV, dA, grad ? 1 : 0);
         ctx.launches++;
+        off += blocks;
     }
+    pac_union::k_union_total<<<1, 256, 0, s>>>(partial, off, acc);
+    ctx.launches++;
     cudaEventRecord(e1, s);
     double h[2];
     cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s);
