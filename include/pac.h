@@ -223,6 +223,24 @@ int pac_union_measure_device(pac_ctx *ctx, const double *d_xyzr, uint32_t n,
                              const pac_complex *cx, double *vol, double *area,
                              double *d_dvol, double *d_darea);
 
+/* Same measure for callers that cannot allocate device memory (for example
+   when a framework's allocator has reserved the GPU's memory, or in a
+   latency-bound loop that cannot take cudaMalloc's implicit
+   synchronisation).  No counterpart in the reference.  All arguments are as
+   for pac_union_measure_device: device balls, a complex with device lists,
+   and device gradient buffers -- both or neither; vol/area are host
+   pointers.  Nothing is allocated: the only scratch is a fixed 2 MiB array
+   inside the library that every GPU loading it holds until exit.
+   Limit: sum over the four lists of ceil(count / 128) <= 65,536 (about 8.4
+   million simplices); larger complexes return PAC_ERR_CAPACITY.  The first
+   call on a device looks up the array's device address; make that first call
+   before any stream capture.  All calls share the one array: calls that
+   overlap on the GPU (two contexts, two streams) race and must be serialised
+   by the caller. */
+int pac_union_measure_noalloc(pac_ctx *ctx, const double *d_xyzr, uint32_t n,
+                              const pac_complex *cx, double *vol, double *area,
+                              double *d_dvol, double *d_darea);
+
 void pac_free_complex(pac_complex *cx);
 void pac_free_batch_complex(pac_batch_complex *cx);
 

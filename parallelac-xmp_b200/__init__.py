@@ -112,6 +112,7 @@ def _lib():
         L.pac_cuda_stream.argtypes = [P]
         L.pac_union_measure.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(Complex), P, P, P, P]
         L.pac_union_measure_device.argtypes = L.pac_union_measure.argtypes
+        L.pac_union_measure_noalloc.argtypes = L.pac_union_measure.argtypes
         L.pac_free_complex.argtypes = [ctypes.POINTER(Complex)]
         L.pac_free_batch_complex.argtypes = [ctypes.POINTER(BatchComplex)]
         L.pac_read_crd.argtypes = [ctypes.c_char_p, ctypes.POINTER(P),
@@ -223,6 +224,16 @@ class Engine:
         alpha_complex_device).  Returns (vol, area)."""
         vol, area = ctypes.c_double(), ctypes.c_double()
         _check(_lib().pac_union_measure_device(
+            self._ctx, ctypes.c_void_p(d_xyzr_ptr), n, ctypes.byref(cx), ctypes.addressof(vol),
+            ctypes.addressof(area), ctypes.c_void_p(d_dvol_ptr or None),
+            ctypes.c_void_p(d_darea_ptr or None)))
+        return vol.value, area.value
+
+    def union_measure_noalloc(self, d_xyzr_ptr, n, cx, d_dvol_ptr=0, d_darea_ptr=0):
+        """As union_measure_device, but nothing is allocated: the library's
+        fixed scratch array is used.  Gradient buffers: both or neither."""
+        vol, area = ctypes.c_double(), ctypes.c_double()
+        _check(_lib().pac_union_measure_noalloc(
             self._ctx, ctypes.c_void_p(d_xyzr_ptr), n, ctypes.byref(cx), ctypes.addressof(vol),
             ctypes.addressof(area), ctypes.c_void_p(d_dvol_ptr or None),
             ctypes.c_void_p(d_darea_ptr or None)))

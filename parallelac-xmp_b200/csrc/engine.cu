@@ -18,6 +18,8 @@ struct pac_ctx {
     pac::Ctx c;
 };
 
+pac::Ctx &pac_ctx_internal(pac_ctx *ctx) { return ctx->c; }
+
 namespace pac {
 
 static thread_local std::string g_last_error;

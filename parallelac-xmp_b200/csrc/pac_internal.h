@@ -82,6 +82,9 @@ int set_error(int status, const std::string &msg);
 
 }  // namespace pac
 
+// The context behind a pac_ctx handle (defined in engine.cu).
+pac::Ctx &pac_ctx_internal(pac_ctx *ctx);
+
 namespace pac_strict {
 int run_pass(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
              pac::PassOutput &out, pac_stats *st);

@@ -30,6 +30,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "pac_internal.h"
@@ -365,3 +366,110 @@ int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uin
 }
 
 }  // namespace pac
+
+// ---------------------------------------------------------------------------
+// pac_union_measure_noalloc: the same measure for callers that cannot
+// allocate device memory.
+//
+// Some callers cannot call cudaMalloc: a process whose device memory is
+// reserved up front by another allocator (a framework's caching pool that
+// owns nearly all of the GPU), or a latency-bound loop that cannot afford
+// cudaMalloc's implicit device synchronisation.  This entry point allocates
+// nothing: the caller passes the balls, the complex and the gradient buffers
+// in device memory, and the only scratch -- one partial (volume, area) sum
+// per block of 128 simplices and the two totals -- lives in the file-scope
+// array below, which every GPU that loads this library holds until the
+// process exits (2 MiB).
+//
+// Limit: the four simplex lists together may need at most kNoAllocBlocks
+// blocks of 128, i.e. sum over vertices, edges, triangles and tetrahedra of
+// ceil(count / 128) <= 65,536 (about 8.4 million simplices); larger
+// complexes are rejected with PAC_ERR_CAPACITY before anything runs.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoAllocBlocks = 65536;
+constexpr int kMaxDevices = 64;
+
+// partial sums (one double4 per block), then one slot for the two totals
+static __device__ __align__(256) double4 g_noalloc_scratch[kNoAllocBlocks + 1];
+
+std::mutex g_noalloc_mutex;
+double4 *g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current).
+// The first call on each device looks it up with cudaGetSymbolAddress; in
+// host code the array's name only stands in for the symbol.
+int noalloc_scratch(int device, double4 **out) {
+    if (device < 0 || device >= kMaxDevices)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return pac::set_error(PAC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
+                                                    cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<double4 *>(ptr);
+    }
+    *out = g_noalloc_ptr[device];
+    return PAC_OK;
+}
+
+}  // namespace
+
+extern "C" int pac_union_measure_noalloc(pac_ctx *ctx, const double *d_xyzr, uint32_t n,
+                                         const pac_complex *cx, double *vol, double *area,
+                                         double *d_dvol, double *d_darea) {
+    if (!ctx || !cx || (n && !d_xyzr))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
+    if ((d_dvol == nullptr) != (d_darea == nullptr))
+        return pac::set_error(PAC_ERR_INVALID_ARG,
+                              "pass both gradient buffers or neither (nothing is allocated)");
+    const uint32_t *lists[4] = {nullptr, cx->edges, cx->tris, cx->tets};
+    const uint64_t counts[4] = {n, cx->n_edges, cx->n_tris, cx->n_tets};
+    uint64_t blocks = 0;
+    for (int k = 0; k < 4; k++) blocks += (counts[k] + 127) / 128;
+    if (blocks > kNoAllocBlocks)
+        return pac::set_error(PAC_ERR_CAPACITY,
+                              "complex too large for pac_union_measure_noalloc: needs " +
+                                  std::to_string(blocks) + " blocks of 128 simplices, the fixed "
+                                  "scratch holds " + std::to_string(kNoAllocBlocks));
+    pac::Ctx &c = pac_ctx_internal(ctx);
+    cudaError_t e = cudaSetDevice(c.device);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    double4 *scratch = nullptr;
+    int rc = noalloc_scratch(c.device, &scratch);
+    if (rc) return rc;
+    cudaStream_t s = c.stream;
+    const bool grad = d_dvol != nullptr;
+    if (grad) {
+        // the gradients accumulate: they must start at zero
+        cudaMemsetAsync(d_dvol, 0, 4 * sizeof(double) * n, s);
+        cudaMemsetAsync(d_darea, 0, 4 * sizeof(double) * n, s);
+    }
+    uint64_t off = 0;
+    for (int k = 1; k <= 4; k++) {
+        if (!counts[k - 1]) continue;
+        unsigned nb = (unsigned)((counts[k - 1] + 127) / 128);
+        pac_union::k_union<<<nb, 128, 0, s>>>(k, counts[k - 1], lists[k - 1],
+                                              reinterpret_cast<const double4 *>(d_xyzr),
+                                              scratch + off, d_dvol, d_darea, grad ? 1 : 0);
+        off += nb;
+    }
+    // every partial slot used is written above; the totals slot is written here
+    double *totals = reinterpret_cast<double *>(scratch + kNoAllocBlocks);
+    pac_union::k_union_total<<<1, 256, 0, s>>>(scratch, off, totals);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    double h[2] = {0, 0};
+    e = cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("union measure: ") + cudaGetErrorString(e));
+    if (vol) *vol = h[0];
+    if (area) *area = h[1];
+    return PAC_OK;
+}

@@ -1,0 +1,53 @@
+"""pac_union_measure_noalloc: the union volume/area measure for callers that
+cannot allocate device memory (a framework whose allocator has reserved the
+GPU, a loop that cannot afford cudaMalloc's implicit synchronisation).  It
+must give what pac_union_measure_device gives, call after call, while using
+only the library's fixed scratch array.
+
+Collected last on purpose (file name), so a failure here leaves every other
+test already run."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SOL, ALPHA = 1.4, 1.0
+
+
+def test_noalloc_matches_allocating_entry_point_twice(pac):
+    import torch
+    balls = pac.globule(3000, seed=pac.SEED_BASE + 41)
+    with pac.Engine(tet_mode="as-written") as eng:
+        d = torch.from_numpy(balls).cuda()
+        cx, _ = eng.alpha_complex_device(d.data_ptr(), len(balls), SOL, ALPHA)
+        x = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
+        dv0 = torch.empty_like(x)
+        da0 = torch.empty_like(x)
+        v0, a0 = eng.union_measure_device(x.data_ptr(), len(balls), cx, dv0.data_ptr(),
+                                          da0.data_ptr())
+        for _ in range(2):  # two calls in a row share the scratch array
+            dv = torch.full_like(x, 7.0)  # stale contents must not leak in
+            da = torch.full_like(x, -3.0)
+            v, a = eng.union_measure_noalloc(x.data_ptr(), len(balls), cx, dv.data_ptr(),
+                                             da.data_ptr())
+            assert abs(v - v0) <= 1e-10 * abs(v0)
+            assert abs(a - a0) <= 1e-10 * abs(a0)
+            assert (dv - dv0).abs().max().item() <= 1e-10 * dv0.abs().max().item()
+            assert (da - da0).abs().max().item() <= 1e-10 * da0.abs().max().item()
+        # totals only, no gradient buffers
+        v, a = eng.union_measure_noalloc(x.data_ptr(), len(balls), cx)
+        assert abs(v - v0) <= 1e-10 * abs(v0) and abs(a - a0) <= 1e-10 * abs(a0)
+
+
+def test_noalloc_rejects_oversized_complex(pac):
+    """Beyond the fixed scratch (65,536 blocks of 128 simplices) the call
+    fails before running anything."""
+    with pac.Engine() as eng:
+        cx = pac.Complex(16, 1, 0, 0, 9_000_000, None, None,
+                         ctypes.cast(ctypes.c_void_p(16), ctypes.POINTER(ctypes.c_uint32)))
+        with pytest.raises(pac.PacError) as ei:
+            eng.union_measure_noalloc(16, 16, cx)
+        assert ei.value.status == -3
+        assert "65536" in str(ei.value)
