@@ -171,6 +171,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_BALLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-molecules", type=int, default=512)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -189,9 +190,13 @@ def main():
 
     pac = ge.load_package()
     n = args.n
-    balls = pac.globule(n, seed=pac.SEED_BASE + 4 + 1000 * rank)
+    # the globule plus 8 isolated corner balls (see pad_corners): every window
+    # centre then lies inside the grid, so the reference can run this input
+    balls = pac.pad_corners(pac.globule(n, seed=pac.SEED_BASE + 4 + 1000 * rank))
+    n = len(balls)
     eng = pac.Engine(device=local, formula="upstream", tet_mode="as-written", predicates="strict")
     d_balls = torch.from_numpy(balls).cuda()
+    torch.cuda.synchronize()  # the engine's stream does not wait on torch's
     stream = torch.cuda.ExternalStream(eng.stream())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
@@ -227,6 +232,7 @@ def main():
     xyzr = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
     dvol = torch.empty((n, 4), dtype=torch.float64, device="cuda")
     darea = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
     cx, _ = eng.alpha_complex_device(d_balls.data_ptr(), n, SOL, ALPHA)
     for _ in range(2):
         eng.union_measure_device(xyzr.data_ptr(), n, cx, dvol.data_ptr(), darea.data_ptr())
@@ -278,6 +284,32 @@ def main():
     achieved = alg_bytes / (tet_ms / 1e3) / 1e9
     traffic = profiled_traffic()
 
+    # ---- batched vs plain per-molecule launches (sample of the 4,096-molecule
+    # batch: sizes log-uniform in [200, 20000], sol 1.4, alpha 0.5)
+    batched = None
+    if args.batch_molecules > 0:
+        sizes = pac.batch_sizes(4096)[:args.batch_molecules]
+        bballs, boff = pac.batch(sizes)
+        eng.alpha_complex_batch(bballs, boff, SOL, 0.5)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        bres, bst = eng.alpha_complex_batch(bballs, boff, SOL, 0.5)
+        t_batch = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        same = True
+        for m in range(len(sizes)):
+            r = eng.alpha_complex(bballs[boff[m]:boff[m + 1]], SOL, 0.5)
+            same = same and r.counts() == bres[m].counts() and \
+                np.array_equal(r.tets, bres[m].tets) and np.array_equal(r.tris, bres[m].tris) and \
+                np.array_equal(r.edges, bres[m].edges)
+        t_plain = time.perf_counter() - t1
+        batched = {"molecules": int(len(sizes)), "balls": int(boff[-1]), "sol_rad": SOL,
+                   "alpha": 0.5, "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
+                   "speedup": t_plain / t_batch, "identical_output": bool(same),
+                   "balls_per_s_batched": float(boff[-1]) / t_batch,
+                   "what": "host C ABI both ways (wall clock): one pac_alpha_complex_batch "
+                           "call vs one pac_alpha_complex call per molecule"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(os.cpu_count() or 1)
@@ -292,8 +324,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "100k-ball globule (0.05/A^3), sol 1.4, alpha 1.0, upstream "
-                               "formulas, orthosphere test applied, strict f32",
+        "config": {"workload": "100k-ball globule (0.05/A^3) + 8 isolated corner balls, sol 1.4, "
+                               "alpha 1.0, upstream formulas, orthosphere test applied, strict f32",
                    "n_balls": n, "sol_rad": SOL, "alpha": ALPHA, "parallelism": "dp%d" % world,
                    "l2": "flushed between steps (256 MB write)"},
         "simplices_per_s": world * (s0["final_edges"] + s0["final_tris"] + s0["final_tets"] + n)
@@ -305,6 +337,7 @@ def main():
                                         "ms_tri_attach", "ms_edge_attach", "ms_emit")},
         "union": {"grad_ms": grad_ms, "volume": uvol, "area": uarea,
                   "what": "volume + area + d/d(centre, radius) of both, FP64, over the final complex"},
+        "batched": batched,
         "e2e": {"value": e2e_value, "unit": "balls/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

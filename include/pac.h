@@ -186,7 +186,11 @@ int pac_alpha_complex(pac_ctx *ctx, const pac_ball *balls, uint32_t n,
                       pac_stats *stats);
 
 /* Same with device-resident input and output (d_balls is a device pointer;
-   out->on_device = 1).  Nothing crosses PCIe except a few counters. */
+   out->on_device = 1).  Nothing crosses PCIe except a few counters.  The
+   engine launches on its own stream (pac_cuda_stream), which does not wait
+   for work on other streams: device inputs must be complete when a device
+   entry point is called (synchronise, or record an event and make the
+   engine's stream wait on it). */
 int pac_alpha_complex_device(pac_ctx *ctx, const pac_ball *d_balls,
                              uint32_t n, float sol_rad, float alpha,
                              pac_complex *out, pac_stats *stats);

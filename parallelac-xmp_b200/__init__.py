@@ -372,6 +372,20 @@ def assembly(nx=8, ny=10, nz=5, per=6250, pitch=60.0, side=57.0, seed=SEED_BASE 
     return out
 
 
+def pad_corners(balls, margin=12.0, radius=1.7):
+    """balls plus 8 isolated balls at the corners of their bounding box grown
+    by `margin` A.  With margin > 2 grid cells the new balls form no
+    simplices, and every window centre of the molecule's simplices falls
+    inside the grid (the reference reads the centre cell without a range
+    check)."""
+    b = np.asarray(balls, dtype=np.float32)
+    lo = b[:, :3].min(0) - margin
+    hi = b[:, :3].max(0) + margin
+    corners = [[(lo, hi)[i][0], (lo, hi)[j][1], (lo, hi)[k][2], radius]
+               for i in (0, 1) for j in (0, 1) for k in (0, 1)]
+    return np.concatenate([b, np.array(corners, np.float32)])
+
+
 def batch_sizes(count=4096, lo=200, hi=20000, seed=SEED_BASE + 3):
     s = np.zeros(count, np.uint32)
     _synth().pac_synth_batch_sizes(seed, count, lo, hi, s.ctypes.data)

@@ -190,6 +190,7 @@ def test_device_entry_point(pac):
     with _engine(pac) as eng:
         host = eng.alpha_complex(balls, 1.4, 1.0)
         d = torch.from_numpy(balls).cuda()
+        torch.cuda.synchronize()
         cx, st = eng.alpha_complex_device(d.data_ptr(), len(balls), 1.4, 1.0)
         assert cx.on_device == 1 and st["kernels_launched"] > 0
         np.testing.assert_array_equal(_device_list(cx.edges, cx.n_edges, 2), host.edges)

@@ -74,6 +74,7 @@ def test_union_gradient_fd_100k_1000_coordinates(pac):
         x = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
         dv = torch.empty_like(x)
         da = torch.empty_like(x)
+        torch.cuda.synchronize()
         eng.union_measure_device(x.data_ptr(), len(balls), cx, dv.data_ptr(), da.data_ptr())
         torch.cuda.synchronize()
         gv, ga = dv.cpu().numpy(), da.cpu().numpy()
@@ -81,12 +82,17 @@ def test_union_gradient_fd_100k_1000_coordinates(pac):
         err_v, err_a = [], []
         for _ in range(1000):
             i, q = int(rng.integers(len(balls))), int(rng.integers(4))
+            # torch writes on its own stream: finish each write before the
+            # engine (which launches on another stream) reads the buffer
             x0 = float(x[i, q])
             x[i, q] = x0 + h
+            torch.cuda.synchronize()
             vp, ap = eng.union_measure_device(x.data_ptr(), len(balls), cx)
             x[i, q] = x0 - h
+            torch.cuda.synchronize()
             vm, am = eng.union_measure_device(x.data_ptr(), len(balls), cx)
             x[i, q] = x0
+            torch.cuda.synchronize()
             err_v.append(abs((vp - vm) / (2 * h) - gv[i, q]) / max(1.0, abs(gv[i, q])))
             err_a.append(abs((ap - am) / (2 * h) - ga[i, q]) / max(1.0, abs(ga[i, q])))
     ev, ea = np.array(err_v), np.array(err_a)

@@ -25,11 +25,13 @@ def test_noalloc_matches_allocating_entry_point_twice(pac):
         x = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
         dv0 = torch.empty_like(x)
         da0 = torch.empty_like(x)
+        torch.cuda.synchronize()  # torch's stream is not the engine's
         v0, a0 = eng.union_measure_device(x.data_ptr(), len(balls), cx, dv0.data_ptr(),
                                           da0.data_ptr())
         for _ in range(2):  # two calls in a row share the scratch array
             dv = torch.full_like(x, 7.0)  # stale contents must not leak in
             da = torch.full_like(x, -3.0)
+            torch.cuda.synchronize()
             v, a = eng.union_measure_noalloc(x.data_ptr(), len(balls), cx, dv.data_ptr(),
                                              da.data_ptr())
             assert abs(v - v0) <= 1e-10 * abs(v0)
