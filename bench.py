@@ -132,15 +132,107 @@ def cpu_baseline(threads):
             "sample": "%d-ball globule, sol 1.4, alpha 1.0, as-written, %.2f s" % (CPU_SAMPLE, dt)}
 
 
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "parallelac-largeData-rr128-nofma")
+REF_SAMPLE = 25_000
+REF_WARM = 1_300
+
+
+def config_of(n):
+    return {"workload": "100k-ball globule (0.05/A^3) + 8 isolated corner balls, sol 1.4, "
+                        "alpha 1.0, upstream formulas, orthosphere test applied, strict f32",
+            "n_balls": n, "sol_rad": SOL, "alpha": ALPHA, "parallelism": "dp1",
+            "l2": "flushed between steps (256 MB write)"}
+
+
+def _ref_run(exe, balls, tmp):
+    """One run of the reference binary: CRD in, output file out; returns its
+    own 'Total time taken (ms)' figure, the wall time and the counts line of
+    the file it wrote."""
+    import re
+    crd, out = os.path.join(tmp, "in.crd"), os.path.join(tmp, "out.txt")
+    with open(crd, "w") as f:
+        f.write("%d\n" % len(balls))
+        for r in balls:
+            f.write("%r %r %r %r\n" % tuple(float(v) for v in r))
+    t0 = time.perf_counter()
+    p = subprocess.run([exe, crd, out, repr(SOL), repr(ALPHA), str(len(balls))],
+                       capture_output=True, text=True, errors="replace", timeout=900)
+    wall = time.perf_counter() - t0
+    m = re.search(r"Total time taken \(ms\):\s*([0-9.]+)", p.stdout)
+    if p.returncode != 0 or not m:
+        raise RuntimeError("reference run failed (rc %d): %s" % (p.returncode, p.stdout[-300:]))
+    with open(out) as f:
+        counts = [int(v) for v in f.readline().split()]
+    return float(m.group(1)), wall, counts
+
+
 def run_reference(args):
+    """The reference arm.  The reference is a CUDA program: its own
+    AlphaComplexLargeData.cu, compiled from its sources by oracle/ref_build.sh
+    with -maxrregcount=128 (built as its CMakeLists.txt says, its orthosphere
+    kernel cannot launch on this GPU and the program aborts) and -fmad=false
+    (so that it computes the same bit-exact complex as this workload), run on
+    the same GPU.  One step = one run of the binary on a 25,000-ball globule
+    sample of the workload (same generator, density, radii, sol-rad, alpha,
+    corner padding); its cost grows slower than linearly with size, so a
+    sample understates its throughput on the full 100k workload somewhat.
+    Before the runs the oracle checks that the sample is one the reference
+    handles safely (every orthosphere window centre inside its grid; no two
+    equal weighted points, on which its simulation of simplicity never ends)
+    and gives the counts that the reference's output must have.  Without the
+    binary (no reference tree where it was built) the oracle port is timed on
+    the host cores instead."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     pac = ge.load_package()
     orc = ge.load_oracle()
+    base = {"impl": "reference", "metric": METRIC, "unit": "balls/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(N_BALLS + 8)}
+    if os.path.exists(REF_EXE):
+        balls = pac.pad_corners(pac.globule(REF_SAMPLE, seed=pac.SEED_BASE + 4))
+        warm = pac.pad_corners(pac.globule(REF_WARM, seed=pac.SEED_BASE))
+        want = {}
+        for name, b in (("sample", balls), ("warm", warm)):
+            e, t, q, st = orc.alpha_complex(b, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True,
+                                            threads=threads)
+            if st["ortho_out_of_grid"] or len(np.unique(b, axis=0)) != len(b):
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "sample outside what the reference handles safely"}))
+                return 0
+            want[name] = [len(b), len(e), len(t), len(q)]
+        with tempfile.TemporaryDirectory() as tmp:
+            for _ in range(args.warmup):
+                _, _, c = _ref_run(REF_EXE, warm, tmp)
+                assert c == want["warm"], (c, want["warm"])
+            ms, walls = [], []
+            for _ in range(args.steps):
+                t, w, c = _ref_run(REF_EXE, balls, tmp)
+                assert c == want["sample"], (c, want["sample"])
+                ms.append(t)
+                walls.append(w)
+        per = sum(ms) / len(ms)
+        v = len(balls) / (per / 1e3)
+        sample = ("%d-ball globule + 8 corner balls per step, one run of the reference "
+                  "binary (-maxrregcount=128 -fmad=false) on this GPU; its own 'Total time "
+                  "taken' (input copy, all kernels, output copy); warm-up runs on a %d-ball "
+                  "globule" % (REF_SAMPLE, REF_WARM))
+        line = dict(base, value=v, ms_per_step=per,
+                    cpu_baseline={"value": v, "unit": "balls/s", "cores": 1,
+                                  "kind": "reference", "sample": sample},
+                    e2e={"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0},
+                    reference={"binary": os.path.basename(REF_EXE), "on": "gpu",
+                               "counts_match_oracle": True, "counts": want["sample"][1:],
+                               "wall_s_per_step": sum(walls) / len(walls)})
+        print(json.dumps(line), flush=True)
+        return 0
+
     balls = pac.globule(CPU_SAMPLE, seed=pac.SEED_BASE + 4)
-    for _ in range(max(args.warmup, 0) and 1):
+    for _ in range(min(args.warmup, 1)):
         orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
     t = []
     for _ in range(args.steps):
@@ -149,16 +241,12 @@ def run_reference(args):
         t.append(time.perf_counter() - t0)
     per = sum(t) / len(t)
     v = CPU_SAMPLE / per
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "balls/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "globule, sol 1.4, alpha 1.0 (CPU sample of %d balls)" % CPU_SAMPLE,
-                       "n_balls": CPU_SAMPLE, "sol_rad": SOL, "alpha": ALPHA},
-            "cpu_baseline": {"value": v, "unit": "balls/s", "cores": threads, "kind": "port",
-                             "sample": "%d-ball globule per step" % CPU_SAMPLE},
-            "e2e": {"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+    sample = "%d-ball globule per step, oracle port on %d host threads" % (CPU_SAMPLE, threads)
+    line = dict(base, value=v, ms_per_step=per * 1e3,
+                cpu_baseline={"value": v, "unit": "balls/s", "cores": threads, "kind": "port",
+                              "sample": sample},
+                e2e={"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
     print(json.dumps(line), flush=True)
     return 0
 
@@ -254,7 +342,11 @@ def main():
     value = world * n / (ms_per_step / 1e3)
 
     # ---- end-to-end through the host C ABI
-    e2e_ms = []
+    # ms_total: CUDA events on the engine's stream from before the input copy
+    # to after the lists have landed in pinned host memory; the host wall time
+    # of the Python call (which also copies the lists into numpy) is reported
+    # beside it
+    e2e_ms, e2e_wall = [], []
     h2d = d2h = 0
     eng.alpha_complex(balls, SOL, ALPHA)
     barrier()
@@ -263,8 +355,8 @@ def main():
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         r = eng.alpha_complex(balls, SOL, ALPHA)
+        e2e_wall.append(time.perf_counter() - t1)
         e2e_ms.append(max(r.stats["ms_total"], 0.0))
-        e2e_wall = time.perf_counter() - t1
         h2d = balls.nbytes
         d2h = r.edges.nbytes + r.tris.nbytes + r.tets.nbytes
     e2e_step = sum(e2e_ms) / len(e2e_ms)
@@ -296,13 +388,13 @@ def main():
         bres, bst = eng.alpha_complex_batch(bballs, boff, SOL, 0.5)
         t_batch = time.perf_counter() - t1
         t1 = time.perf_counter()
-        same = True
-        for m in range(len(sizes)):
-            r = eng.alpha_complex(bballs[boff[m]:boff[m + 1]], SOL, 0.5)
-            same = same and r.counts() == bres[m].counts() and \
-                np.array_equal(r.tets, bres[m].tets) and np.array_equal(r.tris, bres[m].tris) and \
-                np.array_equal(r.edges, bres[m].edges)
+        plain = [eng.alpha_complex(bballs[boff[m]:boff[m + 1]], SOL, 0.5)
+                 for m in range(len(sizes))]
         t_plain = time.perf_counter() - t1
+        same = all(r.counts() == b.counts() and np.array_equal(r.tets, b.tets) and
+                   np.array_equal(r.tris, b.tris) and np.array_equal(r.edges, b.edges)
+                   for r, b in zip(plain, bres))
+        del plain
         batched = {"molecules": int(len(sizes)), "balls": int(boff[-1]), "sol_rad": SOL,
                    "alpha": 0.5, "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
                    "speedup": t_plain / t_batch, "identical_output": bool(same),
@@ -324,10 +416,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "100k-ball globule (0.05/A^3) + 8 isolated corner balls, sol 1.4, "
-                               "alpha 1.0, upstream formulas, orthosphere test applied, strict f32",
-                   "n_balls": n, "sol_rad": SOL, "alpha": ALPHA, "parallelism": "dp%d" % world,
-                   "l2": "flushed between steps (256 MB write)"},
+        "config": dict(config_of(n), parallelism="dp%d" % world),
         "simplices_per_s": world * (s0["final_edges"] + s0["final_tris"] + s0["final_tets"] + n)
         / (ms_per_step / 1e3),
         "complex": {"edges": s0["final_edges"], "tris": s0["final_tris"], "tets": s0["final_tets"],
@@ -339,7 +428,8 @@ def main():
                   "what": "volume + area + d/d(centre, radius) of both, FP64, over the final complex"},
         "batched": batched,
         "e2e": {"value": e2e_value, "unit": "balls/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step},
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step,
+                "host_wall_ms_per_step": 1e3 * sum(e2e_wall) / len(e2e_wall)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k_tets (fused enumeration + alpha + orthosphere)",

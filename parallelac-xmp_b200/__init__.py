@@ -154,7 +154,7 @@ class Engine:
     """A pac_ctx: one CUDA stream and device memory pool on one device."""
 
     def __init__(self, device=0, formula="upstream", tet_mode="as-written", predicates="strict",
-                 order="reference", verbose=False):
+                 order="reference", verbose=False, queue_entries=None):
         L = _lib()
         o = Options()
         L.pac_default_options(ctypes.byref(o))
@@ -164,6 +164,8 @@ class Engine:
         o.predicates = PREDICATES[predicates]
         o.order = ORDER[order]
         o.verbose = int(verbose)
+        if queue_entries:
+            o.reserved_u[0] = int(queue_entries)  # alpha-tetrahedron queue size (testing)
         self._ctx = ctypes.c_void_p()
         _check(L.pac_create(ctypes.byref(self._ctx), ctypes.byref(o)))
 

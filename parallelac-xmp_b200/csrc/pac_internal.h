@@ -40,6 +40,7 @@ struct PipelineConfig {
     int formula;    // pac_formula
     int tet_mode;   // pac_tet_mode
     int verbose;
+    uint64_t queue_entries;  // alpha tetrahedra queued per chunk (24 B each)
 };
 
 // Inputs of one device pass over one or more molecules.

@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
 // tetrahedron survives only if no ball violates its orthosphere.
 constexpr int kQCap = 192;
 
-__device__ __forceinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
+__device__ __noinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
                                               const uint32_t *N, uint32_t key, bool pending,
                                               uint32_t &ball_count) {
     if (pending) {
@@ -765,7 +765,7 @@ __device__ __forceinline__ void emit_survivor(const TetArgs &A, uint64_t p, int 
     mark_face(A.faces, A.loff[v2], (deg2 + 63) >> 6, mb, mc);
 }
 
-constexpr int kLongCap = 32;   // tetrahedra handed to the cooperative scan
+constexpr int kLongCap = 64;   // tetrahedra handed to the cooperative scan
 constexpr int kSerialEvals = 8; // window balls a lane scans alone before handing off
 
 // Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
@@ -773,7 +773,7 @@ constexpr int kSerialEvals = 8; // window balls a lane scans alone before handin
 // then the 26 neighbours range-checked per axis), a prefix sum over the cell
 // sizes flattens the window balls over the lanes.  Returns 1 = violated,
 // 2 = no violation but an exact zero, 0 = empty.
-__device__ __forceinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
+__device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
                                          uint32_t v2, uint32_t v3, uint32_t v4, const float *pa,
                                          const float *pb, const float *pc, const float *pd,
                                          float wa, float wb, float wc, float wd,
@@ -1108,6 +1108,330 @@ __global__ void __launch_bounds__(256, 2) k_tets_ws(TetArgs A) {
     }
 }
 
+// ---- the as-written tetrahedra in two kernels over an HBM queue ----------
+// k_tets_alpha: one warp per ball v1 (balls handed out in order from a
+// counter, over a chunk [lo, hi)).  The candidate fourth vertices of every
+// alpha triangle (v1, v2, v3) are flattened over the lanes (common bits of
+// rows a and b of v1's link matrix, checked against v2's link matrix: the
+// reference's candidate tetrahedra, AlphaComplexLargeData.cu:350-529), each
+// lane applies markRealTets to one candidate, and the passing tetrahedra are
+// appended to the queue with the cell of their orthosphere centre.
+struct TetQueue {
+    uint2 *pk;        // (ball v1, a | b << 8 | c << 16)
+    int4 *cell;       // (gridX, gridY, gridZ, linear centre index)
+    uint64_t cap;
+};
+
+template <int V>
+__global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, uint64_t lo,
+                                                       uint64_t hi) {
+    __shared__ uint16_t smap[8][kMaxDeg];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1;
+    unsigned long long cand_acc = 0, alpha_acc = 0;
+    while (true) {
+        uint64_t p = 0;
+        if (lane == 0) {
+            // stop handing out balls once the queue has overflowed: the chunk
+            // is rerun smaller
+            p = (*(volatile unsigned long long *)&A.ctr[C_SURV] > Q.cap)
+                    ? hi
+                    : lo + atomicAdd(&A.ctr[C_NEXT], 1ull);
+        }
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= hi) break;
+        const uint64_t e0 = A.eoff[p];
+        const int deg = (int)(A.eoff[p + 1] - e0);
+        if (deg < 3) continue;
+        const int W = (deg + 63) >> 6;
+        const uint32_t *N = A.ER + e0;
+        const uint64_t *Lp = A.link + A.loff[p];
+        const Ball B1 = pac::ld_ball(&A.at[p]);
+        const MolGrid G = A.grids[mol_of(A.mol, p)];
+        for (int a = 0; a < deg - 2; a++) {
+            uint64_t ra[kMaxW];
+            int nb = 0;
+#pragma unroll
+            for (int w = 0; w < kMaxW; w++) {
+                ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
+                nb += __popcll(ra[w]);
+            }
+            if (nb < 2) continue;
+            const uint32_t v2 = __ldg(&N[a]);
+            const uint64_t e2 = A.eoff[v2];
+            const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+            const int W2 = (deg2 + 63) >> 6;
+            const uint64_t *L2 = A.link + A.loff[v2];
+            for (int c = a + 1 + lane; c < deg; c += 32) {
+                uint32_t x = __ldg(&N[c]);
+                int pos = lbound(A.ER + e2, deg2, x);
+                smap[wib][c] = (pos < deg2 && __ldg(&A.ER[e2 + pos]) == x) ? (uint16_t)pos
+                                                                           : (uint16_t)0xffff;
+            }
+            __syncwarp();
+            const Ball B2 = pac::ld_ball(&A.at[v2]);
+            for (int k0 = 0; k0 < nb; k0 += 32) {
+                int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
+                uint64_t m[kMaxW];
+                int cnt = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    m[w] = (b >= 0 && w < W) ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
+                                             : 0;
+                    cnt += __popcll(m[w]);
+                }
+                int incl = cnt;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int v = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(kFull, incl, 31);
+                for (int base = 0; base < total; base += 32) {
+                    const int s = base + lane;
+                    int lo2 = 0;
+                    for (int step = 16; step; step >>= 1) {
+                        int v = __shfl_sync(kFull, incl, lo2 + step - 1);
+                        if (v <= s) lo2 += step;
+                    }
+                    const int owner = lo2 & 31;
+                    const int oincl = __shfl_sync(kFull, incl, owner);
+                    const int ocnt = __shfl_sync(kFull, cnt, owner);
+                    const int bo = __shfl_sync(kFull, b, owner);
+                    uint64_t mo[kMaxW];
+#pragma unroll
+                    for (int w = 0; w < kMaxW; w++) {
+                        uint32_t l32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
+                        uint32_t h32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
+                        mo[w] = ((uint64_t)h32 << 32) | l32;
+                    }
+                    bool pass4 = false, passA = false;
+                    int c = -1;
+                    int4 cell = make_int4(0, 0, 0, 0);
+                    if (s < total) {
+                        c = select_bit(mo, W, s - (oincl - ocnt));
+                        const int mb = smap[wib][bo], mc = smap[wib][c];
+                        pass4 = mb != 0xffff && mc != 0xffff &&
+                                ((__ldg(&L2[(uint64_t)mb * W2 + (mc >> 6)]) >> (mc & 63)) & 1ull);
+                        if (pass4) {
+                            const Ball B3 = pac::ld_ball(&A.at[__ldg(&N[bo])]);
+                            const Ball B4 = pac::ld_ball(&A.at[__ldg(&N[c])]);
+                            float4 sphere;
+                            passA = pac::tet_alpha(B1, B2, B3, B4, A.alpha, sphere);
+                            if (passA) {
+                                int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
+                                int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
+                                int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
+                                cell = make_int4(gridX, gridY, gridZ,
+                                                 lin3(gridX, gridY, gridZ, G.gx, G.gy));
+                            }
+                        }
+                    }
+                    const unsigned m4 = __ballot_sync(kFull, pass4);
+                    const unsigned mA = __ballot_sync(kFull, passA);
+                    unsigned long long qbase = 0;
+                    if (lane == 0 && mA) qbase = atomicAdd(&A.ctr[C_SURV], (unsigned long long)__popc(mA));
+                    qbase = __shfl_sync(kFull, qbase, 0);
+                    if (passA) {
+                        uint64_t pos = qbase + __popc(mA & lt_mask);
+                        if (pos < Q.cap) {
+                            Q.pk[pos] = make_uint2((uint32_t)p, (uint32_t)a | ((uint32_t)bo << 8) |
+                                                                    ((uint32_t)c << 16));
+                            Q.cell[pos] = cell;
+                        }
+                    }
+                    if (lane == 0) {
+                        cand_acc += __popc(m4);
+                        alpha_acc += __popc(mA);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        bump(A.ctr, C_CAND_Q, cand_acc);
+        bump(A.ctr, C_ALPHA_Q, alpha_acc);
+    }
+}
+
+// k_tets_scan: the empty-orthosphere test (checkTetsOrthosphere,
+// AlphaComplexLargeData.cu:606-734) of the queued tetrahedra.  Each lane
+// owns one tetrahedron at a time and evaluates one window ball per step; a
+// warp claims 32 queue entries at a time and a lane takes the next unclaimed
+// one as soon as its own is decided.  A tetrahedron still open after
+// kSerialEvals balls is handed to the cooperative test (the whole warp scans
+// its window), so no lane runs a long window alone.  Survivors are recorded
+// and mark their faces.
+__global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
+                                                      unsigned long long *claim) {
+    __shared__ uint32_t lkey[8][kLongCap];
+    __shared__ uint32_t lball[8][kLongCap];
+    __shared__ int4 lcell[8][kLongCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1;
+    unsigned long long evals = 0, oob = 0;
+    uint64_t head = 0, tail = 0;  // this warp's claimed range (warp-uniform)
+    bool have = false, more = true;
+    uint32_t p = 0, key = 0, v2 = 0, v3 = 0, v4 = 0;
+    float pa[3], pb[3], pc[3], pd[3], wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
+    int gX = 0, gY = 0, gZ = 0, q = 0, nev = 0;
+    int4 mycell = make_int4(0, 0, 0, 0);
+    uint32_t e = 0, end = 0;
+    bool zero = false;
+    int ln = 0;
+    const MolGrid *G = A.grids;
+    auto flush_long = [&]() {
+        for (int t = 0; t < ln; t++) {
+            const uint32_t k2 = lkey[wib][t], p2 = lball[wib][t];
+            const int4 cl = lcell[wib][t];
+            const uint32_t *N2 = A.ER + A.eoff[p2];
+            const uint32_t u2 = __ldg(&N2[k2 & 0xff]), u3 = __ldg(&N2[(k2 >> 8) & 0xff]),
+                           u4 = __ldg(&N2[(k2 >> 16) & 0xff]);
+            const Ball a1 = pac::ld_ball(&A.at[p2]), a2 = pac::ld_ball(&A.at[u2]),
+                       a3 = pac::ld_ball(&A.at[u3]), a4 = pac::ld_ball(&A.at[u4]);
+            float qa[3], qb[3], qc[3], qd[3];
+            qa[0] = a1.x, qa[1] = a1.y, qa[2] = a1.z;
+            qb[0] = a2.x, qb[1] = a2.y, qb[2] = a2.z;
+            qc[0] = a3.x, qc[1] = a3.y, qc[2] = a3.z;
+            qd[0] = a4.x, qd[1] = a4.y, qd[2] = a4.z;
+            const float xa = a1.r * a1.r, xb = a2.r * a2.r, xc = a3.r * a3.r, xd = a4.r * a4.r;
+            const float ori = pac::orient3d(qa, qb, qc, qd);
+            const MolGrid G2 = A.grids[mol_of(A.mol, p2)];
+            int r = coop_test(A, G2, p2, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc, xd, ori, cl, evals);
+            if (r != 1 && lane == 0) {
+                const int deg = (int)(A.eoff[p2 + 1] - A.eoff[p2]);
+                uint32_t dummy = 0;
+                emit_survivor(A, p2, (deg + 63) >> 6, A.loff[p2], N2, k2, r == 2, dummy);
+                if (r != 2) atomicAdd(&A.tcount[p2], 1u);
+            }
+        }
+        ln = 0;
+        __syncwarp();
+    };
+    while (true) {
+        // claim: idle lanes take the next entries of the warp's range
+        unsigned want = __ballot_sync(kFull, !have);
+        if (want && head >= tail && more) {
+            uint64_t b = 0;
+            if (lane == 0) b = atomicAdd(claim, 32ull);
+            b = __shfl_sync(kFull, b, 0);
+            head = b;
+            tail = min(nq, b + 32);
+            if (head >= tail) more = false;
+        }
+        if (want && head < tail) {
+            int r = __popc(want & lt_mask);
+            if (!have && head + r < tail) {
+                uint64_t idx = head + r;
+                uint2 pk = Q.pk[idx];
+                int4 cl = Q.cell[idx];
+                p = pk.x;
+                key = pk.y;
+                G = A.grids + mol_of(A.mol, p);
+                const uint32_t *N = A.ER + A.eoff[p];
+                v2 = __ldg(&N[key & 0xff]);
+                v3 = __ldg(&N[(key >> 8) & 0xff]);
+                v4 = __ldg(&N[(key >> 16) & 0xff]);
+                const Ball a1 = pac::ld_ball(&A.at[p]), a2 = pac::ld_ball(&A.at[v2]),
+                           a3 = pac::ld_ball(&A.at[v3]), a4 = pac::ld_ball(&A.at[v4]);
+                pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = a1.r * a1.r;
+                pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
+                pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
+                pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
+                orientation = pac::orient3d(pa, pb, pc, pd);
+                gX = cl.x;
+                gY = cl.y;
+                gZ = cl.z;
+                mycell = cl;
+                q = 0;
+                nev = 0;
+                zero = false;
+                if (cl.w >= 0 && (uint64_t)cl.w < G->ncell) {
+                    uint64_t gc = G->cell_base + (uint64_t)cl.w;
+                    e = A.cellbeg[gc];
+                    end = A.cellbeg[gc + 1];
+                } else {
+                    e = end = 0;
+                    oob++;
+                }
+                have = true;
+            }
+            head = min(tail, head + (uint64_t)__popc(want));
+        }
+        if (!__any_sync(kFull, have)) {
+            if (!more || ln) {
+                flush_long();
+                if (!more) break;
+            }
+            continue;
+        }
+        const bool handoff = have && nev >= kSerialEvals;
+        const unsigned hm = __ballot_sync(kFull, handoff);
+        if (hm) {
+            int pos = ln + __popc(hm & lt_mask);
+            if (handoff && pos < kLongCap) {
+                lkey[wib][pos] = key;
+                lball[wib][pos] = p;
+                lcell[wib][pos] = mycell;
+                have = false;
+            }
+            ln = min(kLongCap, ln + __popc(hm));
+            if (ln > kLongCap - 32) {
+                __syncwarp();
+                flush_long();
+            }
+        }
+        if (!have) continue;
+        if (e < end) {
+            uint32_t x = e++;
+            if (x == p || x == v2 || x == v3 || x == v4) continue;
+            const Ball atom = pac::ld_ball(&A.at[x]);
+            float pe[3];
+            pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
+            float we = atom.r * atom.r;
+            evals++;
+            nev++;
+            float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+            bool viol = orientation < 0 ? (result < 0) : (result > 0);
+            if (viol) {
+                have = false;
+                continue;
+            }
+            if (result == 0) zero = true;
+            continue;
+        }
+        bool found = false;
+        const int Ggx = G->gx, Ggy = G->gy, Ggz = G->gz;
+        while (q < 26 && !found) {
+            q++;
+            int rr = q - 1 + (q >= 14 ? 1 : 0);
+            int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
+            int zz = (int)((unsigned)gZ + (unsigned)i), yy = (int)((unsigned)gY + (unsigned)j),
+                xx = (int)((unsigned)gX + (unsigned)k);
+            if ((zz >= Ggz) || (yy >= Ggy) || (xx >= Ggx)) continue;
+            if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+            uint64_t gc = G->cell_base + (uint64_t)lin3(xx, yy, zz, Ggx, Ggy);
+            e = A.cellbeg[gc];
+            end = A.cellbeg[gc + 1];
+            found = true;
+        }
+        if (!found) {
+            const uint32_t *N = A.ER + A.eoff[p];
+            const int deg = (int)(A.eoff[p + 1] - A.eoff[p]);
+            uint32_t dummy = 0;
+            emit_survivor(A, p, (deg + 63) >> 6, A.loff[p], N, key, zero, dummy);
+            if (!zero) atomicAdd(&A.tcount[p], 1u);
+            have = false;
+        }
+    }
+    evals = warp_sum(evals);
+    oob = warp_sum(oob);
+    if (lane == 0) {
+        bump(A.ctr, C_INSPHERE, evals);
+        bump(A.ctr, C_OOB, oob);
+    }
+}
+
 // Tetrahedra whose window holds an insphere value of exactly 0: the test
 // again, with the reference's simulation of simplicity for those balls
 // (AlphaComplexLargeData.cu:645-652, 659-667).
@@ -1353,6 +1677,191 @@ __global__ void __launch_bounds__(256) k_tri_final(uint64_t n, const float4 *__r
                             int pos = lbound(ER + e1, deg1, v2);
                             if (pos < deg1 && ER[e1 + pos] == v2) eflag[e1 + pos] = 1;
                         }
+                    }
+                }
+            }
+        }
+        if (lane == 0) tricount[p] = count;
+    }
+    oob = warp_sum(oob);
+    if (lane == 0) bump(ctr, C_OOB, oob);
+}
+
+// Final triangles with work stealing (same decisions as k_tri_final): one
+// warp per ball v1, balls handed out from a counter.  The alpha triangles
+// of v1 that are not tetrahedron faces are queued in shared memory row by
+// row; each lane takes one, recomputes its orthosphere (markRealTriangles)
+// and tests one window ball per step (checkDanglingTris,
+// AlphaComplexLargeData.cu:798-872), taking the next queued triangle as soon
+// as its own is decided.  An unattached triangle sets its bit in `faces`.
+// Then the warp counts v1's final triangles and marks their edges.
+constexpr int kTQCap = 256;
+
+template <int V>
+__global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 *__restrict__ at,
+                                                       const uint64_t *__restrict__ eoff,
+                                                       const uint32_t *__restrict__ ER,
+                                                       const uint64_t *__restrict__ loff,
+                                                       const uint64_t *__restrict__ link,
+                                                       uint64_t *faces, uint32_t *tricount,
+                                                       uint8_t *eflag, const uint32_t *cellbeg,
+                                                       const uint32_t *mol, const MolGrid *grids,
+                                                       float alpha, unsigned long long *ctr) {
+    __shared__ uint16_t qa[8][kTQCap], qb[8][kTQCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1;
+    unsigned long long oob = 0;
+    while (true) {
+        uint64_t p = 0;
+        if (lane == 0) p = atomicAdd(&ctr[C_NEXT], 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= n) break;
+        const uint64_t e0 = eoff[p];
+        const int deg = (int)(eoff[p + 1] - e0);
+        uint32_t count = 0;
+        if (deg >= 2) {
+            const int W = (deg + 63) >> 6;
+            const uint32_t *N = ER + e0;
+            const uint64_t lp = loff[p];
+            const Ball A0 = pac::ld_ball(&at[p]);
+            const MolGrid *G = grids + mol_of(mol, p);
+            int row = 0;       // next row to queue (warp-uniform)
+            uint64_t rbits[kMaxW];  // unqueued candidate bits of `row`
+            bool rloaded = false;
+            // lane state
+            bool have = false;
+            int ta = 0, tb = 0;
+            uint32_t v1 = 0, v2 = 0;
+            float px = 0, py = 0, pz = 0, cur = 0;
+            int gX = 0, gY = 0, gZ = 0, q = 0;
+            uint32_t e = 0, end = 0;
+            int qn = 0, head = 0;  // shared queue (warp-uniform)
+            while (true) {
+                // refill the queue from the remaining rows
+                if (head >= qn) {
+                    qn = 0;
+                    head = 0;
+                    while (row < deg - 1 && qn < kTQCap - 64) {
+                        if (!rloaded) {
+#pragma unroll
+                            for (int w = 0; w < kMaxW; w++)
+                                rbits[w] = w < W ? (link[lp + (uint64_t)row * W + w] &
+                                                    ~faces[lp + (uint64_t)row * W + w])
+                                                 : 0;
+                            rloaded = true;
+                        }
+                        int nc = 0;
+#pragma unroll
+                        for (int w = 0; w < kMaxW; w++) nc += __popcll(rbits[w]);
+                        int take = min(nc, kTQCap - qn);
+                        for (int k0 = 0; k0 < take; k0 += 32) {
+                            int k = k0 + lane;
+                            if (k < take) {
+                                qa[wib][qn + k] = (uint16_t)row;
+                                qb[wib][qn + k] = (uint16_t)select_bit(rbits, W, k);
+                            }
+                        }
+                        qn += take;
+                        if (take == nc) {
+                            row++;
+                            rloaded = false;
+                        } else {
+                            // drop the queued bits from the row, keep the rest
+                            for (int k = 0; k < take; k++) {
+                                int b = select_bit(rbits, W, 0);
+                                rbits[b >> 6] &= ~(1ull << (b & 63));
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+                unsigned want = __ballot_sync(kFull, !have);
+                if (want && head < qn) {
+                    int r = __popc(want & lt_mask);
+                    if (!have && head + r < qn) {
+                        ta = qa[wib][head + r];
+                        tb = qb[wib][head + r];
+                        v1 = N[ta];
+                        v2 = N[tb];
+                        float4 p1;
+                        pac::tri_alpha<V>(A0, pac::ld_ball(&at[v1]), pac::ld_ball(&at[v2]), alpha,
+                                          p1);
+                        px = p1.x;
+                        py = p1.y;
+                        pz = p1.z;
+                        cur = p1.w;
+                        gX = pac::cell_coord(p1.x, G->minx, G->step);
+                        gY = pac::cell_coord(p1.y, G->miny, G->step);
+                        gZ = pac::cell_coord(p1.z, G->minz, G->step);
+                        int cc = lin3(gX, gY, gZ, G->gx, G->gy);
+                        q = 0;
+                        if (cc >= 0 && (uint64_t)cc < G->ncell) {
+                            e = cellbeg[G->cell_base + cc];
+                            end = cellbeg[G->cell_base + cc + 1];
+                        } else {
+                            e = end = 0;
+                            oob++;
+                        }
+                        have = true;
+                    }
+                    head = min(qn, head + __popc(want));
+                }
+                if (!__any_sync(kFull, have)) {
+                    if (head >= qn && row >= deg - 1) break;
+                    continue;
+                }
+                if (!have) continue;
+                if (e < end) {
+                    uint32_t x = e++;
+                    if (x == (uint32_t)p || x == v1 || x == v2) continue;
+                    if (pac::attached(pac::ld_ball(&at[x]), px, py, pz, cur)) have = false;
+                    continue;
+                }
+                bool found = false;
+                const int Ggx = G->gx, Ggy = G->gy, Ggz = G->gz;
+                while (q < 26 && !found) {
+                    q++;
+                    int rr = q - 1 + (q >= 14 ? 1 : 0);
+                    int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
+                    int zz = (int)((unsigned)gZ + (unsigned)i), yy = (int)((unsigned)gY + (unsigned)j),
+                        xx = (int)((unsigned)gX + (unsigned)k);
+                    if ((zz >= Ggz) || (yy >= Ggy) || (xx >= Ggx)) continue;
+                    if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
+                    uint64_t gc = G->cell_base + (uint64_t)lin3(xx, yy, zz, Ggx, Ggy);
+                    e = cellbeg[gc];
+                    end = cellbeg[gc + 1];
+                    found = true;
+                }
+                if (!found) {
+                    atomicOr((unsigned long long *)&faces[lp + (uint64_t)ta * W + (tb >> 6)],
+                             1ull << (tb & 63));
+                    have = false;
+                }
+            }
+            __syncwarp();
+            __threadfence_block();
+            // count the final triangles and mark their edges
+            for (int a = 0; a < deg - 1; a++) {
+                uint64_t fin[kMaxW];
+                int nf = 0;
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    fin[w] = w < W ? faces[lp + (uint64_t)a * W + w] : 0;
+                    nf += __popcll(fin[w]);
+                }
+                count += nf;
+                if (!nf) continue;
+                if (lane == 0) eflag[e0 + a] = 1;
+                const uint32_t va = N[a];
+                const uint64_t e1 = eoff[va];
+                const int deg1 = (int)(eoff[va + 1] - e1);
+                for (int k0 = 0; k0 < nf; k0 += 32) {
+                    int b = (k0 + lane < nf) ? select_bit(fin, W, k0 + lane) : -1;
+                    if (b >= 0) {
+                        eflag[e0 + b] = 1;
+                        const uint32_t vb = N[b];
+                        int pos = lbound(ER + e1, deg1, vb);
+                        if (pos < deg1 && ER[e1 + pos] == vb) eflag[e1 + pos] = 1;
                     }
                 }
             }
@@ -1673,39 +2182,105 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         k_tets<V, 2><<<warp_blocks(n), 256, 0, s>>>(T);
         LAUNCH_CHECK(ctx);
     } else {
-        uint64_t cap = std::max<uint64_t>(1024, 16 * n);
-        for (int attempt = 0; attempt < 2; attempt++) {
-            T.surv = ar.alloc_n<uint2>(cap);
-            T.surv_cap = cap;
-            T.pend = ar.alloc_n<uint2>(cap / 4 + 1024);
-            T.pend_cap = cap / 4 + 1024;
-            if (!T.surv || !T.pend) return PAC_ERR_OOM;
-            CK(cudaMemsetAsync(ctr + C_CAND_Q, 0, 2 * sizeof(unsigned long long), s));
-            CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
-            CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
-            CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
-            CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
-            k_tets_ws<V><<<std::min<unsigned>(warp_blocks(n), 148 * 2), 256, 0, s>>>(T);
+        // queue of alpha tetrahedra in HBM, processed in chunks of balls
+        const uint64_t qcap = std::max<uint64_t>(1 << 16, cfg.queue_entries);
+        TetQueue Q;
+        Q.pk = ar.alloc_n<uint2>(qcap);
+        Q.cell = ar.alloc_n<int4>(qcap);
+        Q.cap = qcap;
+        uint64_t scap = std::max<uint64_t>(1024, 16 * n);
+        T.surv = ar.alloc_n<uint2>(scap);
+        T.surv_cap = scap;
+        T.pend = ar.alloc_n<uint2>(scap / 4 + 1024);
+        T.pend_cap = scap / 4 + 1024;
+        unsigned long long *claim = ar.alloc_n<unsigned long long>(1);
+        unsigned long long *ctrA = ar.alloc_n<unsigned long long>(C_NCOUNTERS);
+        if (!Q.pk || !Q.cell || !T.surv || !T.pend || !claim || !ctrA) return PAC_ERR_OOM;
+        CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
+        CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
+        CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
+        CK(cudaMemsetAsync(T.tcount, 0, sizeof(uint32_t) * n, s));
+        unsigned long long cand_total = 0, alpha_total = 0;
+        uint64_t lo = 0, chunk = n;
+        while (lo < n) {
+            const uint64_t hi = std::min<uint64_t>(n, lo + chunk);
+            TetArgs TA = T;
+            TA.ctr = ctrA;
+            CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
+            k_tets_alpha<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 2), 256, 0, s>>>(TA, Q,
+                                                                                          lo, hi);
             LAUNCH_CHECK(ctx);
-            unsigned long long sp[2];
-            CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(sp), cudaMemcpyDeviceToHost, s));
+            unsigned long long ha[C_NCOUNTERS], used[2];
+            CK(cudaMemcpyAsync(ha, ctrA, sizeof(ha), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(used, ctr + C_SURV, sizeof(used), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            uint64_t need = std::max<uint64_t>(sp[0] + sp[1], 4 * sp[1]);
-            if (sp[0] + sp[1] <= cap && sp[1] <= T.pend_cap) {
-                if (sp[1]) {
-                    k_sos_resolve<<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
-                    LAUNCH_CHECK(ctx);
-                    CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(unsigned long long),
-                                       cudaMemcpyDeviceToHost, s));
-                    CK(cudaStreamSynchronize(s));
-                }
-                nQ = sp[0];
-                break;
+            const unsigned long long queued = ha[C_SURV];
+            if (queued > qcap) {
+                if (hi - lo == 1)
+                    return pac::set_error(PAC_ERR_CAPACITY,
+                                          "the alpha tetrahedra of one ball exceed the queue");
+                chunk = std::max<uint64_t>(1, (uint64_t)((double)(hi - lo) * 0.5));
+                continue;
             }
-            if (attempt == 1)
-                return pac::set_error(PAC_ERR_CAPACITY, "tetrahedron buffer overflow");
-            cap = need + 1024;
+            // every queued tetrahedron becomes at most one survivor or one
+            // pending entry: grow either list (keeping its entries) first
+            if (used[0] + queued > T.surv_cap) {
+                const uint64_t nc = std::max<uint64_t>(2 * T.surv_cap, used[0] + queued);
+                uint2 *nb = ar.alloc_n<uint2>(nc);
+                if (!nb) return PAC_ERR_OOM;
+                if (used[0])
+                    CK(cudaMemcpyAsync(nb, T.surv, sizeof(uint2) * used[0],
+                                       cudaMemcpyDeviceToDevice, s));
+                T.surv = nb;
+                T.surv_cap = nc;
+            }
+            if (used[1] + queued > T.pend_cap) {
+                const uint64_t nc = std::max<uint64_t>(2 * T.pend_cap, used[1] + queued);
+                uint2 *nb = ar.alloc_n<uint2>(nc);
+                if (!nb) return PAC_ERR_OOM;
+                if (used[1])
+                    CK(cudaMemcpyAsync(nb, T.pend, sizeof(uint2) * used[1],
+                                       cudaMemcpyDeviceToDevice, s));
+                T.pend = nb;
+                T.pend_cap = nc;
+            }
+            cand_total += ha[C_CAND_Q];
+            alpha_total += ha[C_ALPHA_Q];
+            CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
+            k_tets_scan<<<148 * 4, 256, 0, s>>>(T, Q, queued, claim);
+            LAUNCH_CHECK(ctx);
+            // next chunk sized from this one's queue fill
+            if (queued)
+                chunk = std::max<uint64_t>(
+                    1, (uint64_t)(0.85 * (double)qcap * (double)(hi - lo) / (double)queued));
+            else
+                chunk = n;
+            lo = hi;
         }
+        {
+            unsigned long long cq[2] = {cand_total, alpha_total};
+            CK(cudaMemcpyAsync(ctr + C_CAND_Q, cq, sizeof(cq), cudaMemcpyHostToDevice, s));
+        }
+        unsigned long long sp[2];
+        CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(sp), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (sp[0] > T.surv_cap || sp[1] > T.pend_cap)
+            return pac::set_error(PAC_ERR_CAPACITY, "tetrahedron survivor buffer overflow");
+        if (sp[1] && sp[0] + sp[1] > T.surv_cap) {  // resolved entries join the survivors
+            uint2 *nb = ar.alloc_n<uint2>(sp[0] + sp[1]);
+            if (!nb) return PAC_ERR_OOM;
+            if (sp[0])
+                CK(cudaMemcpyAsync(nb, T.surv, sizeof(uint2) * sp[0], cudaMemcpyDeviceToDevice, s));
+            T.surv = nb;
+            T.surv_cap = sp[0] + sp[1];
+        }
+        if (sp[1]) {
+            k_sos_resolve<<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
+            LAUNCH_CHECK(ctx);
+            CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        nQ = sp[0];
         rc = exclusive_scan(ctx, T.tcount, n, toff);
         if (rc) return rc;
     }
@@ -1716,8 +2291,9 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     uint64_t *tpos = ar.alloc_n<uint64_t>(n + 1);
     uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
     if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
-    k_tri_final<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, loff, link, faces, tricount,
-                                                  eflag, cellbeg, mol, grids, in.alpha, ctr);
+    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(n), 148 * 3), 256, 0, s>>>(
+        n, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids, in.alpha, ctr);
     LAUNCH_CHECK(ctx);
     tm.mark();  // 5
     k_edge_final<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, eflag, cellbeg, mol, grids,

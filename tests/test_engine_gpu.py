@@ -260,14 +260,32 @@ def test_engine_matches_reference_digest_5000(pac):
 
 def test_fma_flavour_against_reference_default_contraction(pac):
     """The contraction flavour against the reference built with nvcc's
-    default -fmad=true (rr128): the number of differing simplices on 1k4c is
-    recorded in the test output; the strict flavour differs from that build
-    in 22 simplices."""
+    default -fmad=true (rr128) on 1k4c.  Which multiply-adds nvcc fuses
+    depends on the code around each expression, so no build of different
+    kernels can match that binary bit for bit; the flavour is the closer
+    approximation: fewer differing simplices than the strict flavour
+    (which differs from that build in 82 of ~118k)."""
     balls = golden("1k4c_plain_alpha1")[0]
     E, T, Q = _refrun("1k4c_a1", "rr128")
-    with _engine(pac, 0, "as-written", "fma") as eng:
-        r = eng.alpha_complex(balls, 0.0, 1.0)
-    diff = sum(len(set(map(tuple, canonical(a))) ^ set(map(tuple, canonical(b))))
-               for a, b in ((r.edges, E), (r.tris, T), (r.tets, Q)))
-    print("fma flavour vs reference default build: %d differing simplices" % diff)
-    assert diff <= 22
+
+    def diff(pred):
+        with _engine(pac, 0, "as-written", pred) as eng:
+            r = eng.alpha_complex(balls, 0.0, 1.0)
+        return [len(set(map(tuple, canonical(a))) ^ set(map(tuple, canonical(b))))
+                for a, b in ((r.edges, E), (r.tris, T), (r.tets, Q))]
+    fma, strict = diff("fma"), diff("strict")
+    print("vs the reference's default-contraction build, differing (edges, tris, tets): "
+          "fma flavour %s, strict flavour %s" % (fma, strict))
+    assert sum(strict) == 82
+    assert sum(fma) < sum(strict)
+
+
+def test_chunked_tetrahedron_queue(pac, orc):
+    """A queue far smaller than the alpha tetrahedra of the pass: the balls
+    are processed in many chunks (with overflow retries); same lists."""
+    balls = pac.globule(4000, seed=pac.SEED_BASE + 12)
+    e, t, q, st = orc.alpha_complex(balls, 1.4, 1.0, orc.UPSTREAM, tet_ortho=True)
+    with pac.Engine(tet_mode="as-written", queue_entries=200_000) as eng:
+        r = eng.alpha_complex(balls, 1.4, 1.0)
+    _same(r, e, t, q)
+    assert r.stats["alpha_tets"] == st["alpha_tets"] and r.stats["cand_tets"] == st["cand_tets"]
