@@ -152,11 +152,20 @@ static void big_mul(big *r, const big *a, const big *b) {
     if (big_sign(&y) < 0) { big_neg(&y); s = -s; }
     uint32_t acc[BL];
     memset(acc, 0, sizeof(acc));
-    for (int i = 0; i < BL; i++) {
+    int nx = BL, ny = BL; /* limbs in use (magnitudes are non-negative now) */
+    while (nx > 0 && !x.w[nx - 1]) nx--;
+    while (ny > 0 && !y.w[ny - 1]) ny--;
+    for (int i = 0; i < nx; i++) {
         if (!x.w[i]) continue;
         uint64_t c = 0;
-        for (int j = 0; i + j < BL; j++) {
+        int j = 0;
+        for (; j < ny && i + j < BL; j++) {
             uint64_t t = (uint64_t)x.w[i] * y.w[j] + acc[i + j] + c;
+            acc[i + j] = (uint32_t)t;
+            c = t >> 32;
+        }
+        for (; c && i + j < BL; j++) { /* carry out of the top limb */
+            uint64_t t = (uint64_t)acc[i + j] + c;
             acc[i + j] = (uint32_t)t;
             c = t >> 32;
         }
@@ -211,7 +220,7 @@ static void to_big(big *r, float f, int scale) {
 }
 
 /* Load the five points in SoS (sorted-index) order at one common scale. */
-static void sos_load(sos_pts *s, float *const *ip, const float *iw) {
+static void sos_load(sos_pts *s, float *const *ip, const float *iw, int radii) {
     int emin = 0, emax = -1000;
     for (int i = 0; i < 5; i++) {
         for (int k = 0; k < 4; k++) {
@@ -237,7 +246,13 @@ static void sos_load(sos_pts *s, float *const *ip, const float *iw) {
             big_add(&t, &s->lift[i], &sq);
             s->lift[i] = t;
         }
-        to_big(&s->w2[i], iw[i], 2 * emin);
+        if (radii) { /* iw holds radii: the weight is their exact square */
+            big r;
+            to_big(&r, iw[i], emin);
+            big_mul(&s->w2[i], &r, &r);
+        } else {
+            to_big(&s->w2[i], iw[i], 2 * emin);
+        }
         big_sub(&t, &s->lift[i], &s->w2[i]);
         s->lift[i] = t;
     }
@@ -371,10 +386,21 @@ static int sos_minor(const sos_pts *s, int d) {
     return big_sign(&t);
 }
 
+static int sos4_impl(const float *p0, const float *p1, const float *p2,
+                     const float *p3, const float *p4, float w0, float w1,
+                     float w2, float w3, float w4, int i0, int i1, int i2,
+                     int i3, int i4, int radii, int *depth_out);
 int orc_sos4(const float *p0, const float *p1, const float *p2,
              const float *p3, const float *p4, float w0, float w1, float w2,
              float w3, float w4, int i0, int i1, int i2, int i3, int i4,
              int *depth_out) {
+    return sos4_impl(p0, p1, p2, p3, p4, w0, w1, w2, w3, w4, i0, i1, i2, i3,
+                     i4, 0, depth_out);
+}
+static int sos4_impl(const float *p0, const float *p1, const float *p2,
+                     const float *p3, const float *p4, float w0, float w1,
+                     float w2, float w3, float w4, int i0, int i1, int i2,
+                     int i3, int i4, int radii, int *depth_out) {
     /* bubble sort of the indices recording the swap parity (PRED:4676-4707) */
     int idx[5] = {i0, i1, i2, i3, i4}, ord[5] = {0, 1, 2, 3, 4};
     int swaps = 0;
@@ -394,7 +420,7 @@ int orc_sos4(const float *p0, const float *p1, const float *p2,
         iw[i] = ws[ord[i]];
     }
     sos_pts s;
-    sos_load(&s, ip, iw);
+    sos_load(&s, ip, iw, radii);
     int sign = 0, d;
     for (d = 1; d <= 48 && !sign; d++) sign = sos_minor(&s, d);
     d--;
@@ -411,11 +437,122 @@ int orc_sos4(const float *p0, const float *p1, const float *p2,
 }
 
 /* ------------------------------------------------------------------ */
+/* Decision-exact predicates (ORC_EXACT): exact_oracle.cpp evaluates     */
+/* them (extended-precision filter, then arbitrary-precision integers);  */
+/* here the balls are handed over as (x, y, z, r) rows.                  */
+int oex_edge(const float *b, float alpha);
+int oex_tri(const float *b, float alpha);
+int oex_tet(const float *b, float alpha);
+int oex_orient(const float *b);
+int oex_insphere(const float *b);
+int oex_edge_attached(const float *b);
+int oex_tri_attached(const float *b);
+#define ORC_XV 2 /* internal formula code of the exact mode */
+
+static void x_rows(float *b, const oatom *const *a, int k) {
+    for (int i = 0; i < k; i++) {
+        b[4 * i] = a[i]->x; b[4 * i + 1] = a[i]->y;
+        b[4 * i + 2] = a[i]->z; b[4 * i + 3] = a[i]->r;
+    }
+}
+static int x_edge(const oatom *a1, const oatom *a2, float alpha) {
+    const oatom *a[2] = {a1, a2};
+    float b[8];
+    x_rows(b, a, 2);
+    return oex_edge(b, alpha);
+}
+static int x_tri(const oatom *a1, const oatom *a2, const oatom *a3, float alpha) {
+    const oatom *a[3] = {a1, a2, a3};
+    float b[12];
+    x_rows(b, a, 3);
+    return oex_tri(b, alpha);
+}
+static int x_tet(const oatom *a1, const oatom *a2, const oatom *a3, const oatom *a4,
+                 float alpha, int *flat) {
+    const oatom *a[4] = {a1, a2, a3, a4};
+    float b[16];
+    x_rows(b, a, 4);
+    int r = oex_tet(b, alpha);
+    *flat = r == 2;
+    return r != 0;
+}
+/* s[0..nv-1]: the simplex (nv = 2 or 3); q: the other ball */
+static int x_attached(const oatom *const *s, int nv, const oatom *q) {
+    const oatom *a[4] = {s[0], s[1], nv == 3 ? s[2] : q, q};
+    float b[16];
+    x_rows(b, a, nv + 1);
+    return nv == 2 ? oex_edge_attached(b) : oex_tri_attached(b);
+}
+static int x_orient(const oatom *pa, const oatom *pb, const oatom *pc, const oatom *pd) {
+    const oatom *a[4] = {pa, pb, pc, pd};
+    float b[16];
+    x_rows(b, a, 4);
+    return oex_orient(b);
+}
+static int x_insphere(const oatom *const *a5) {
+    float b[20];
+    x_rows(b, a5, 5);
+    return oex_insphere(b);
+}
+
+/* FP64 window centres of the exact mode (the decisions do not use them);
+   the engine computes the same double operations in the same order. */
+static void x_edge_centre(const oatom *a1, const oatom *a2, float *c) {
+    const double ux = (double)a2->x - a1->x, uy = (double)a2->y - a1->y,
+                 uz = (double)a2->z - a1->z;
+    const double uu = ux * ux + uy * uy + uz * uz;
+    const double w1 = (double)a1->r * a1->r, w2 = (double)a2->r * a2->r;
+    const double t = (uu + w1 - w2) / (2.0 * uu);
+    c[0] = (float)(a1->x + t * ux);
+    c[1] = (float)(a1->y + t * uy);
+    c[2] = (float)(a1->z + t * uz);
+}
+static void x_tri_centre(const oatom *a1, const oatom *a2, const oatom *a3, float *c) {
+    const double ux = (double)a2->x - a1->x, uy = (double)a2->y - a1->y,
+                 uz = (double)a2->z - a1->z;
+    const double vx = (double)a3->x - a1->x, vy = (double)a3->y - a1->y,
+                 vz = (double)a3->z - a1->z;
+    const double nx = uy * vz - uz * vy, ny = uz * vx - ux * vz, nz = ux * vy - uy * vx;
+    const double w1 = (double)a1->r * a1->r;
+    const double B2 = ux * ux + uy * uy + uz * uz + w1 - (double)a2->r * a2->r;
+    const double B3 = vx * vx + vy * vy + vz * vz + w1 - (double)a3->r * a3->r;
+    const double cx = B2 * (vy * nz - vz * ny) + B3 * (ny * uz - nz * uy);
+    const double cy = B2 * (vz * nx - vx * nz) + B3 * (nz * ux - nx * uz);
+    const double cz = B2 * (vx * ny - vy * nx) + B3 * (nx * uy - ny * ux);
+    const double k = 1.0 / (2.0 * (nx * nx + ny * ny + nz * nz));
+    c[0] = (float)(a1->x + cx * k);
+    c[1] = (float)(a1->y + cy * k);
+    c[2] = (float)(a1->z + cz * k);
+}
+static void x_tet_centre(const oatom *a1, const oatom *a2, const oatom *a3,
+                         const oatom *a4, float *c) {
+    const double ux = (double)a2->x - a1->x, uy = (double)a2->y - a1->y,
+                 uz = (double)a2->z - a1->z;
+    const double vx = (double)a3->x - a1->x, vy = (double)a3->y - a1->y,
+                 vz = (double)a3->z - a1->z;
+    const double sx = (double)a4->x - a1->x, sy = (double)a4->y - a1->y,
+                 sz = (double)a4->z - a1->z;
+    const double w1 = (double)a1->r * a1->r;
+    const double B2 = ux * ux + uy * uy + uz * uz + w1 - (double)a2->r * a2->r;
+    const double B3 = vx * vx + vy * vy + vz * vz + w1 - (double)a3->r * a3->r;
+    const double B4 = sx * sx + sy * sy + sz * sz + w1 - (double)a4->r * a4->r;
+    const double vsx = vy * sz - vz * sy, vsy = vz * sx - vx * sz, vsz = vx * sy - vy * sx;
+    const double sux = sy * uz - sz * uy, suy = sz * ux - sx * uz, suz = sx * uy - sy * ux;
+    const double uvx = uy * vz - uz * vy, uvy = uz * vx - ux * vz, uvz = ux * vy - uy * vx;
+    const double d = ux * vsx + uy * vsy + uz * vsz;
+    const double k = 1.0 / (2.0 * d);
+    c[0] = (float)(a1->x + (B2 * vsx + B3 * sux + B4 * uvx) * k);
+    c[1] = (float)(a1->y + (B2 * vsy + B3 * suy + B4 * uvy) * k);
+    c[2] = (float)(a1->z + (B2 * vsz + B3 * suz + B4 * uvz) * k);
+}
+
+/* ------------------------------------------------------------------ */
 /* Reference-formula filters                                            */
 
 /* markRealEdges: LD:167-190 (upstream), PLAIN:203-230 (plain-xmp) */
 static int edge_alpha(const oatom *a1, const oatom *a2, float alpha,
                       int variant) {
+    if (variant == ORC_XV) return x_edge(a1, a2, alpha);
     float a = a1->x - a2->x;
     float b = a1->y - a2->y;
     float c = a1->z - a2->z;
@@ -441,6 +578,12 @@ static int edge_alpha(const oatom *a1, const oatom *a2, float alpha,
    Writes the orthosphere (X, Y, Z, power). */
 static int tri_alpha(const oatom *a1, const oatom *a2, const oatom *a3,
                      float alpha, int variant, float *ortho) {
+    if (variant == ORC_XV) {
+        int m = x_tri(a1, a2, a3, alpha);
+        ortho[0] = ortho[1] = ortho[2] = ortho[3] = 0.0f;
+        if (m) x_tri_centre(a1, a2, a3, ortho);
+        return m;
+    }
     float a11 = a1->x - a2->x, a12 = a1->y - a2->y, a13 = a1->z - a2->z;
     float b1 = (a1->x * a1->x - a2->x * a2->x) + (a1->y * a1->y - a2->y * a2->y);
     b1 = b1 + (a1->z * a1->z - a2->z * a2->z);
@@ -506,7 +649,13 @@ static int tri_alpha(const oatom *a1, const oatom *a2, const oatom *a3,
 
 /* markRealTets: LD:531-591 (identical in both variants) */
 static int tet_alpha(const oatom *a1, const oatom *a2, const oatom *a3,
-                     const oatom *a4, float alpha, float *ortho) {
+                     const oatom *a4, float alpha, int variant, float *ortho) {
+    if (variant == ORC_XV) {
+        int flat, m = x_tet(a1, a2, a3, a4, alpha, &flat);
+        ortho[0] = ortho[1] = ortho[2] = ortho[3] = 0.0f;
+        if (m && !flat) x_tet_centre(a1, a2, a3, a4, ortho);
+        return m;
+    }
     float a11 = a1->x - a2->x, a12 = a1->y - a2->y, a13 = a1->z - a2->z;
     float b1 = (a1->x * a1->x - a2->x * a2->x) + (a1->y * a1->y - a2->y * a2->y);
     b1 = b1 + (a1->z * a1->z - a2->z * a2->z);
@@ -615,6 +764,7 @@ typedef struct {
     float pa[3], pb[3], pc[3], pd[3];
     float wa, wb, wc, wd;
     float orientation;
+    int exact;
     uint64_t evals, sos, sos_exh;
 } tet_ctx;
 
@@ -627,15 +777,26 @@ static int tet_visit(void *vctx, uint32_t a) {
     float pe[3] = {e->x, e->y, e->z};
     float we = e->r * e->r;
     t->evals++;
-    float res = orc_insphere_w(t->pa, t->pb, t->pc, t->pd, pe, t->wa, t->wb,
-                               t->wc, t->wd, we);
+    float res;
+    if (t->exact) {
+        const oatom *a5[5] = {&t->at[t->v[0]], &t->at[t->v[1]], &t->at[t->v[2]],
+                              &t->at[t->v[3]], e};
+        res = (float)x_insphere(a5);
+    } else {
+        res = orc_insphere_w(t->pa, t->pb, t->pc, t->pd, pe, t->wa, t->wb,
+                             t->wc, t->wd, we);
+    }
     if (res == 0.0f) {
         int depth;
         t->sos++;
-        res = (float)orc_sos4(t->pa, t->pb, t->pc, t->pd, pe, t->wa, t->wb,
-                              t->wc, t->wd, we, (int)t->at[t->v[0]].idx,
-                              (int)t->at[t->v[1]].idx, (int)t->at[t->v[2]].idx,
-                              (int)t->at[t->v[3]].idx, (int)e->idx, &depth);
+        /* exact mode: the weights are the radii squared exactly */
+        res = (float)sos4_impl(
+            t->pa, t->pb, t->pc, t->pd, pe,
+            t->exact ? t->at[t->v[0]].r : t->wa, t->exact ? t->at[t->v[1]].r : t->wb,
+            t->exact ? t->at[t->v[2]].r : t->wc, t->exact ? t->at[t->v[3]].r : t->wd,
+            t->exact ? e->r : we, (int)t->at[t->v[0]].idx, (int)t->at[t->v[1]].idx,
+            (int)t->at[t->v[2]].idx, (int)t->at[t->v[3]].idx, (int)e->idx,
+            t->exact, &depth);
         if (depth == 49) t->sos_exh++;
     }
     if (t->orientation < 0) return res < 0;
@@ -646,6 +807,7 @@ typedef struct {
     const oatom *at;
     uint32_t v[3];
     int nv;
+    int exact;
     float px, py, pz, cur;
 } att_ctx;
 
@@ -656,6 +818,11 @@ static int att_visit(void *vctx, uint32_t a) {
     for (int i = 0; i < t->nv; i++)
         if (a == t->v[i]) return 0;
     const oatom *e = &t->at[a];
+    if (t->exact) {
+        const oatom *sv[3] = {&t->at[t->v[0]], &t->at[t->v[1]],
+                              t->nv == 3 ? &t->at[t->v[2]] : NULL};
+        return x_attached(sv, t->nv, e);
+    }
     float dx = e->x - t->px, dy = e->y - t->py, dz = e->z - t->pz;
     float pw = dx * dx + dy * dy;
     pw = pw + dz * dz;
@@ -713,6 +880,8 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
     (void)threads;
 #endif
     if (n == 0) return 0;
+    const int exact = (flags & ORC_EXACT) != 0;
+    if (exact) variant = ORC_XV;
     /* ---- input, bounding box (LD:1078-1111) ---- */
     oatom *in = XMALLOC(oatom, n);
     float minx = 0, miny = 0, minz = 0, maxx = 0, maxy = 0, maxz = 0;
@@ -899,7 +1068,7 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
                     if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0)
                         continue;
                     c++;
-                    ca += tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, o4);
+                    ca += tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4);
                 }
             }
             g0 = g1;
@@ -928,7 +1097,7 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
                     if (find2(T2, T3, b, e, v3, v4) < 0) continue;
                     if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0) continue;
                     float o4[4];
-                    if (tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, o4)) {
+                    if (tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4)) {
                         Q[4 * o] = i; Q[4 * o + 1] = v2;
                         Q[4 * o + 2] = v3; Q[4 * o + 3] = v4;
                         memcpy(&QO[4 * o], o4, 16);
@@ -956,7 +1125,9 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
         t.pb[0] = a2->x; t.pb[1] = a2->y; t.pb[2] = a2->z; t.wb = a2->r * a2->r;
         t.pc[0] = a3->x; t.pc[1] = a3->y; t.pc[2] = a3->z; t.wc = a3->r * a3->r;
         t.pd[0] = a4->x; t.pd[1] = a4->y; t.pd[2] = a4->z; t.wd = a4->r * a4->r;
-        t.orientation = orc_orient3d(t.pa, t.pb, t.pc, t.pd);
+        t.exact = exact;
+        t.orientation = exact ? (float)x_orient(a1, a2, a3, a4)
+                              : orc_orient3d(t.pa, t.pb, t.pc, t.pd);
         t.evals = t.sos = t.sos_exh = 0;
         int viol = window_visit(&g, QO[4 * q], QO[4 * q + 1], QO[4 * q + 2],
                                 tet_visit, &t, &oob);
@@ -1013,6 +1184,7 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
         t.at = at;
         t.v[0] = T1[k]; t.v[1] = T2[k]; t.v[2] = T3[k];
         t.nv = 3;
+        t.exact = exact;
         t.px = TO[4 * k]; t.py = TO[4 * k + 1]; t.pz = TO[4 * k + 2];
         t.cur = TO[4 * k + 3];
         tkeep[k] = !window_visit(&g, t.px, t.py, t.pz, att_visit, &t, &oob);
@@ -1082,6 +1254,12 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
         cur = cur + ez * ez;
         cur = cur - (a1->r * a1->r);
         t.cur = cur;
+        t.exact = exact;
+        if (exact) {
+            float c[3];
+            x_edge_centre(a1, a2, c);
+            t.px = c[0]; t.py = c[1]; t.pz = c[2];
+        }
         ekeep[k] = !window_visit(&g, t.px, t.py, t.pz, att_visit, &t, &oob);
     }
     uint64_t nEk = 0;
@@ -1124,4 +1302,17 @@ void orc_free(orc_result *res) {
     free(res->tris);
     free(res->tets);
     res->edges = res->tris = res->tets = NULL;
+}
+
+int orc_exact_pred(int kind, const float *b, float alpha) {
+    switch (kind) {
+    case 0: return oex_edge(b, alpha);
+    case 1: return oex_tri(b, alpha);
+    case 2: return oex_tet(b, alpha);
+    case 3: return oex_orient(b);
+    case 4: return oex_insphere(b);
+    case 5: return oex_edge_attached(b);
+    case 6: return oex_tri_attached(b);
+    }
+    return -9;
 }

@@ -28,7 +28,14 @@ enum {
        that kernel needs more registers than a 512-thread block can hold
        (161 per thread for sm_100a), its launch fails, and every
        alpha-filtered tetrahedron is kept. */
-    ORC_TET_ORTHO = 1
+    ORC_TET_ORTHO = 1,
+    /* Decision-exact predicates: every edge/triangle/tetrahedron alpha
+       test, orientation, insphere and attachment test is the exact sign of
+       its polynomial in the binary32 inputs (weights r^2 exact), evaluated
+       in multi-word integers; windows are centred at FP64 orthocentres.
+       The formula variant does not matter in this mode.  status = -6 when
+       an input's range exceeds the integers' width. */
+    ORC_EXACT = 2
 };
 
 typedef struct {
@@ -63,6 +70,13 @@ float orc_orient3d(const float *pa, const float *pb, const float *pc,
 float orc_insphere_w(const float *pa, const float *pb, const float *pc,
                      const float *pd, const float *pe, float wa, float wb,
                      float wc, float wd, float we);
+/* Single decision-exact predicates on balls (x, y, z, r) with weights
+   r^2 (see ORC_EXACT): kind 0 edge alpha (2 balls), 1 triangle alpha (3),
+   2 tetrahedron alpha (4; 2 when flat), 3 orient3d sign (4), 4 insphere
+   sign (5), 5 edge attached by the last ball (3), 6 triangle attached by
+   the last ball (4).  Returns the decision (0/1/2) or the sign. */
+int orc_exact_pred(int kind, const float *balls, float alpha);
+
 /* returns the SoS sign (+1/-1); *depth receives the SoS depth reached */
 int orc_sos4(const float *p0, const float *p1, const float *p2,
              const float *p3, const float *p4, float w0, float w1, float w2,

@@ -15,6 +15,7 @@ REF_PRED_PATH = os.path.join(HERE, "_ref", "libpredref.so")
 
 UPSTREAM, PLAIN_XMP = 0, 1
 TET_ORTHO = 1  # flag: apply the empty-orthosphere test as written
+EXACT = 2      # flag: decision-exact predicates (multi-word integers)
 
 
 class _Res(ctypes.Structure):
@@ -55,6 +56,8 @@ def lib():
         L.orc_sos4.restype = ctypes.c_int
         L.orc_sos4.argtypes = [f3] * 5 + [ctypes.c_float] * 5 + [ctypes.c_int] * 5 + [
             ctypes.POINTER(ctypes.c_int)]
+        L.orc_exact_pred.restype = ctypes.c_int
+        L.orc_exact_pred.argtypes = [ctypes.c_int, f3, ctypes.c_float]
         _LIB = L
     return _LIB
 
@@ -65,15 +68,19 @@ def _take(ptr, count, k):
     return np.ctypeslib.as_array(ptr, (count * k,)).reshape(count, k).copy()
 
 
-def alpha_complex(balls, sol_rad, alpha, variant=UPSTREAM, tet_ortho=True, threads=0):
-    """Returns (edges, tris, tets, stats) in the reference binary's order."""
+def alpha_complex(balls, sol_rad, alpha, variant=UPSTREAM, tet_ortho=True, threads=0,
+                  exact=False):
+    """Returns (edges, tris, tets, stats) in the reference binary's order.
+    exact=True: decision-exact predicates instead of the reference's
+    single-precision formulas."""
     b = np.ascontiguousarray(balls, dtype=np.float32)
     r = _Res()
+    flags = (TET_ORTHO if tet_ortho else 0) | (EXACT if exact else 0)
     rc = lib().orc_alpha_complex(b.ctypes.data_as(ctypes.c_void_p), len(b), float(sol_rad),
-                                 float(alpha), variant, TET_ORTHO if tet_ortho else 0, threads,
-                                 ctypes.byref(r))
-    if rc != 0:
-        raise RuntimeError("oracle failed: %d" % rc)
+                                 float(alpha), variant, flags, threads, ctypes.byref(r))
+    if rc != 0 or r.status != 0:
+        lib().orc_free(ctypes.byref(r))
+        raise RuntimeError("oracle failed: %d / status %d" % (rc, r.status))
     try:
         E, T, Q = _take(r.edges, r.n_edges, 2), _take(r.tris, r.n_tris, 3), _take(r.tets, r.n_tets, 4)
         st = {k: int(getattr(r, k)) for k in
@@ -108,6 +115,18 @@ def sos4(pts, ws, idx):
     s = lib().orc_sos4(*[k[1] for k in keep], *[float(w) for w in ws], *[int(i) for i in idx],
                        ctypes.byref(d))
     return s, d.value
+
+
+def exact_pred(kind, balls, alpha=0.0):
+    """One decision-exact predicate on up to five balls (x, y, z, r), weights
+    r^2: kind 0 edge alpha, 1 triangle alpha, 2 tetrahedron alpha (2 when
+    flat), 3 orient3d sign, 4 insphere sign, 5 edge attached by ball 2,
+    6 triangle attached by ball 3."""
+    b = np.zeros((5, 4), np.float32)
+    a = np.asarray(balls, np.float32)
+    b[:len(a)] = a
+    return lib().orc_exact_pred(int(kind), b.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                float(alpha))
 
 
 def canonical(a):
