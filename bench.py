@@ -314,7 +314,8 @@ def main():
             stats.append(st)
         barrier()
         wall = time.perf_counter() - t0
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    dev_ms = sum(step_ms)
 
     # ---- union volume/area and their gradients on the final complex
     xyzr = torch.from_numpy(pac.grown_radii(balls, SOL, ALPHA)).cuda()
@@ -399,6 +400,10 @@ def main():
                    "alpha": 0.5, "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
                    "speedup": t_plain / t_batch, "identical_output": bool(same),
                    "balls_per_s_batched": float(boff[-1]) / t_batch,
+                   "batched_engine_ms": bst["ms_total"],
+                   "batched_stage_ms": {k: round(bst[k], 3) for k in
+                                        ("ms_h2d", "ms_grid", "ms_edges", "ms_tris", "ms_tets",
+                                         "ms_tri_attach", "ms_edge_attach", "ms_emit", "ms_d2h")},
                    "what": "host C ABI both ways (wall clock): one pac_alpha_complex_batch "
                            "call vs one pac_alpha_complex call per molecule"}
 
@@ -438,6 +443,10 @@ def main():
         "gpu_launches": int(sum(s["kernels_launched"] for s in stats)),
         "clocks": clocks,
         "wall_s": wall,
+        # per timed step: CUDA events around the call, and the engine's own
+        # events from its first to its last operation on the stream
+        "step_ms": [round(x, 3) for x in step_ms],
+        "engine_ms": [round(s_["ms_total"], 3) for s_ in stats],
     }
     print(json.dumps(line), flush=True)
     eng.close()

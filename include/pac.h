@@ -83,9 +83,18 @@ typedef enum {
        FMA contraction is compiled with contraction enabled (nvcc -fmad=true),
        to follow the reference binary built with default flags. */
     PAC_PRED_REFCOMPAT_FMA = 1,
-    /* Exact decisions: a double-precision semi-static filter for each
-       orientation/power/attachment test and an exact multi-word integer
-       evaluation for the cases the filter cannot decide. */
+    /* Exact decisions (no counterpart in the reference, which has no
+       working exact fallback): every edge/triangle/tetrahedron alpha test,
+       orientation, insphere and attachment test is the exact sign of its
+       polynomial in the binary32 inputs, weights (r + sol)^2 taken exactly.
+       Each is decided by a double-precision filter with a running error
+       bound, and by 640-bit integer arithmetic when the filter cannot tell
+       (pac_stats.filter_evals / exact_fallbacks).  Exact zeros of insphere
+       go to the simulation of simplicity as in the reference.  Candidate
+       sets and windows are the reference's; window centres are computed in
+       double precision.  The formula option has no effect.  Inputs whose
+       binary exponents span too widely for the integers give
+       PAC_ERR_EXACT_RANGE. */
     PAC_PRED_EXACT = 2
 } pac_pred_mode;
 

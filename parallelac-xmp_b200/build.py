@@ -59,7 +59,7 @@ def build(verbose=False, ptxas_info=False):
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     jobs = [
         (os.path.join(OBJ, "pipeline_strict.o"),
-         [NVCC] + NVFLAGS + extra + ["-fmad=false", "-DPAC_NS=pac_strict", "-c",
+         [NVCC] + NVFLAGS + extra + ["-fmad=false", "-DPAC_NS=pac_strict", "-DPAC_WITH_EXACT=1", "-c",
                                      os.path.join(SRC, "pipeline.cu")],
          [os.path.join(SRC, "pipeline.cu")] + hdrs),
         (os.path.join(OBJ, "pipeline_fma.o"),

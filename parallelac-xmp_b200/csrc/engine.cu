@@ -116,7 +116,8 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
     cudaMemGetInfo(&freeb, &totalb);
     uint64_t qbytes = std::min<uint64_t>(freeb / 4, 8ull << 30);
     if (c.opt.reserved_u[0]) qbytes = c.opt.reserved_u[0] * 24ull;  // test hook: entries
-    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 24};
+    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 24,
+                            c.opt.predicates == PAC_PRED_EXACT};
     pac::PassInput in{d_balls, n, n_mol, h_off, sol, alpha};
     int rc = (c.opt.predicates == PAC_PRED_REFCOMPAT_FMA)
                  ? pac_fma::run_pass(c, cfg, in, out, st)
@@ -134,11 +135,9 @@ int validate_opts(const pac_options &o) {
         return pac::set_error(PAC_ERR_INVALID_ARG, "unknown formula");
     if (o.tet_mode != PAC_TETS_AS_WRITTEN && o.tet_mode != PAC_TETS_AS_RUN)
         return pac::set_error(PAC_ERR_INVALID_ARG, "unknown tet_mode");
-    if (o.predicates != PAC_PRED_REFCOMPAT && o.predicates != PAC_PRED_REFCOMPAT_FMA)
-        return pac::set_error(PAC_ERR_INVALID_ARG,
-                              o.predicates == PAC_PRED_EXACT
-                                  ? "PAC_PRED_EXACT is not available in this build"
-                                  : "unknown predicate mode");
+    if (o.predicates != PAC_PRED_REFCOMPAT && o.predicates != PAC_PRED_REFCOMPAT_FMA &&
+        o.predicates != PAC_PRED_EXACT)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "unknown predicate mode");
     if (o.order != PAC_ORDER_REFERENCE && o.order != PAC_ORDER_CANONICAL)
         return pac::set_error(PAC_ERR_INVALID_ARG, "unknown order");
     return PAC_OK;

@@ -41,6 +41,7 @@ struct PipelineConfig {
     int tet_mode;   // pac_tet_mode
     int verbose;
     uint64_t queue_entries;  // alpha tetrahedra queued per chunk (24 B each)
+    bool exact;              // decision-exact predicates (strict flavour only)
 };
 
 // Inputs of one device pass over one or more molecules.

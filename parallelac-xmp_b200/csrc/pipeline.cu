@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "exactpred.cuh"
 #include "pac_internal.h"
 #include "refarith.cuh"
 #include "sos.cuh"
@@ -47,7 +48,8 @@ constexpr unsigned kFull = 0xffffffffu;
 // device-side counters (one slot each)
 enum Counter {
     C_CAND_E, C_ALPHA_E, C_CAND_T, C_ALPHA_T, C_CAND_Q, C_ALPHA_Q, C_INSPHERE, C_SOS,
-    C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NEXT, C_NCOUNTERS
+    C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NEXT, C_FILTER, C_FALLBACK,
+    C_NCOUNTERS
 };
 
 struct MolGrid {
@@ -131,6 +133,149 @@ __device__ __forceinline__ void bump(unsigned long long *ctr, int which, unsigne
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
     return v;
+}
+
+// ------------------------------------------------------------------ decisions
+// Each test of the pipeline in one of two arithmetics: the reference's
+// single-precision formulas (V = kUpstream, kPlainXmp; refarith.cuh) or the
+// decision-exact cascade (V = kExact; exactpred.cuh).  In the exact mode the
+// "weight" slots of the insphere/orientation helpers carry radii, squared
+// exactly inside the predicates.
+using pac::ex::Tally;
+
+template <int V>
+__device__ __forceinline__ float wt(float r) {
+    if constexpr (V == pac::kExact) return r;
+    else return r * r;
+}
+
+template <int V>
+__device__ __forceinline__ bool dec_edge(const Ball a, const Ball b, float alpha, Tally &t) {
+    if constexpr (V == pac::kExact) return pac::ex::edge_alpha(a, b, alpha, t);
+    else return pac::edge_alpha<V>(a, b, alpha);
+}
+
+// alpha mark of a triangle; the orthosphere (centre, power) goes to o
+template <int V>
+__device__ __forceinline__ bool dec_tri(const Ball a, const Ball b, const Ball c, float alpha,
+                                        float4 &o, Tally &t) {
+    if constexpr (V == pac::kExact) {
+        o = make_float4(0.f, 0.f, 0.f, 0.f);
+        return pac::ex::tri_alpha(a, b, c, alpha, t);
+    } else {
+        return pac::tri_alpha<V>(a, b, c, alpha, o);
+    }
+}
+
+// window centre (and the reference's power) of an alpha triangle
+template <int V>
+__device__ __forceinline__ float4 tri_sphere(const Ball a, const Ball b, const Ball c, float alpha) {
+    if constexpr (V == pac::kExact) {
+        const float3 q = pac::ex::tri_centre(a, b, c);
+        return make_float4(q.x, q.y, q.z, 0.f);
+    } else {
+        float4 o;
+        pac::tri_alpha<V>(a, b, c, alpha, o);
+        return o;
+    }
+}
+
+// alpha mark of a tetrahedron; its orthosphere centre goes to o (zeros when
+// the tetrahedron is flat, as in the reference)
+template <int V>
+__device__ __forceinline__ bool dec_tet(const Ball a, const Ball b, const Ball c, const Ball d,
+                                        float alpha, float4 &o, Tally &t) {
+    if constexpr (V == pac::kExact) {
+        bool flat = false;
+        const bool m = pac::ex::tet_alpha(a, b, c, d, alpha, flat, t);
+        o = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m && !flat) {
+            const float3 q = pac::ex::tet_centre(a, b, c, d);
+            o = make_float4(q.x, q.y, q.z, 0.f);
+        }
+        return m;
+    } else {
+        return pac::tet_alpha(a, b, c, d, alpha, o);
+    }
+}
+
+template <int V>
+__device__ __forceinline__ float dec_orient(const float *pa, const float *pb, const float *pc,
+                                            const float *pd, float wa, float wb, float wc, float wd,
+                                            Tally &t) {
+    if constexpr (V == pac::kExact)
+        return (float)pac::ex::orient_sign(Ball{pa[0], pa[1], pa[2], wa}, Ball{pb[0], pb[1], pb[2], wb},
+                                           Ball{pc[0], pc[1], pc[2], wc}, Ball{pd[0], pd[1], pd[2], wd}, t);
+    else
+        return pac::orient3d(pa, pb, pc, pd);
+}
+
+template <int V>
+__device__ __forceinline__ float dec_insphere(const float *pa, const float *pb, const float *pc,
+                                              const float *pd, const float *pe, float wa, float wb,
+                                              float wc, float wd, float we, Tally &t) {
+    if constexpr (V == pac::kExact)
+        return (float)pac::ex::insphere_sign(
+            Ball{pa[0], pa[1], pa[2], wa}, Ball{pb[0], pb[1], pb[2], wb}, Ball{pc[0], pc[1], pc[2], wc},
+            Ball{pd[0], pd[1], pd[2], wd}, Ball{pe[0], pe[1], pe[2], we}, t);
+    else
+        return pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+}
+
+// Attachment of the triangle (a0, v1, v2) by ball q; (px, py, pz, cur) is
+// the reference's orthosphere of the triangle (unused in the exact mode).
+template <int V>
+__device__ __forceinline__ bool dec_tri_attached(const Ball a0, const float4 *at, uint32_t v1,
+                                                 uint32_t v2, const Ball q, float px, float py,
+                                                 float pz, float cur, Tally &t) {
+    if constexpr (V == pac::kExact)
+        return pac::ex::tri_attached(a0, pac::ld_ball(&at[v1]), pac::ld_ball(&at[v2]), q, t);
+    else
+        return pac::attached(q, px, py, pz, cur);
+}
+
+// Window centre of an alpha edge and the reference's power there.
+template <int V>
+__device__ __forceinline__ void edge_sphere(const Ball a1, const Ball a2, float &px, float &py,
+                                            float &pz, float &cur) {
+    if constexpr (V == pac::kExact) {
+        const float3 c = pac::ex::edge_centre(a1, a2);
+        px = c.x, py = c.y, pz = c.z, cur = 0.f;
+    } else {
+        pac::edge_foot(a1, a2, px, py, pz, cur);
+    }
+}
+
+template <int V>
+__device__ __forceinline__ bool dec_edge_attached(const Ball a1, const Ball a2, const Ball q,
+                                                  float px, float py, float pz, float cur,
+                                                  Tally &t) {
+    if constexpr (V == pac::kExact) return pac::ex::edge_attached(a1, a2, q, t);
+    else return pac::attached(q, px, py, pz, cur);
+}
+
+// End of a warp-per-ball kernel (all lanes present): add the lanes'
+// tallies to the counters.
+template <int V>
+__device__ __forceinline__ void flush_tally(const Tally &t, unsigned long long *ctr) {
+    if constexpr (V == pac::kExact) {
+        const unsigned long long e = warp_sum(t.evals), f = warp_sum(t.fallbacks);
+        const bool r = __any_sync(kFull, t.range != 0);
+        if ((threadIdx.x & 31) == 0) {
+            bump(ctr, C_FILTER, e);
+            bump(ctr, C_FALLBACK, f);
+            if (r) bump(ctr, C_SOS_RANGE, 1);
+        }
+    }
+}
+// The same from a single thread.
+template <int V>
+__device__ __forceinline__ void flush_tally_thread(const Tally &t, unsigned long long *ctr) {
+    if constexpr (V == pac::kExact) {
+        if (t.evals) atomicAdd(&ctr[C_FILTER], (unsigned long long)t.evals);
+        if (t.fallbacks) atomicAdd(&ctr[C_FALLBACK], (unsigned long long)t.fallbacks);
+        if (t.range) atomicAdd(&ctr[C_SOS_RANGE], 1ull);
+    }
 }
 
 // ------------------------------------------------------------------ scan
@@ -347,6 +492,7 @@ __global__ void __launch_bounds__(256) k_edges(uint64_t n, const float4 *__restr
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
+    Tally tally;
     for (uint64_t p = warp; p < n; p += nwarps) {
         const MolGrid G = grids[mol_of(mol, p)];
         int cell = (int)(cellof[p] - G.cell_base);
@@ -394,7 +540,7 @@ __global__ void __launch_bounds__(256) k_edges(uint64_t n, const float4 *__restr
             uint32_t l = 0;
             if (act) {
                 l = sbeg + (s - (sinc - scnt));
-                pass = pac::edge_alpha<V>(A, pac::ld_ball(&at[l]), alpha);
+                pass = dec_edge<V>(A, pac::ld_ball(&at[l]), alpha, tally);
             }
             unsigned m = __ballot_sync(kFull, pass);
             if (FILL && pass) ER[out + kept + __popc(m & ((1u << lane) - 1))] = l;
@@ -406,6 +552,7 @@ __global__ void __launch_bounds__(256) k_edges(uint64_t n, const float4 *__restr
             alpha_acc += kept;
         }
     }
+    if (!FILL) flush_tally<V>(tally, ctr);
     if (!FILL && lane == 0) {
         bump(ctr, C_CAND_E, cand_acc);
         bump(ctr, C_ALPHA_E, alpha_acc);
@@ -438,6 +585,7 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
+    Tally tally;
     for (uint64_t p = warp; p < n; p += nwarps) {
         const uint64_t e0 = eoff[p];
         const int deg = (int)(eoff[p + 1] - e0);
@@ -462,7 +610,7 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
                     cand = pos < deg1 && __ldg(&N1[pos]) == v2;
                     if (cand) {
                         float4 o;
-                        pass = pac::tri_alpha<V>(A, A1, pac::ld_ball(&at[v2]), alpha, o);
+                        pass = dec_tri<V>(A, A1, pac::ld_ball(&at[v2]), alpha, o, tally);
                     }
                 }
                 unsigned cm = __ballot_sync(kFull, cand), pm = __ballot_sync(kFull, pass);
@@ -480,6 +628,7 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
         }
         if (lane < W) L[(uint64_t)(deg - 1) * W + lane] = 0;
     }
+    flush_tally<V>(tally, ctr);
     if (lane == 0) {
         bump(ctr, C_CAND_T, cand_acc);
         bump(ctr, C_ALPHA_T, alpha_acc);
@@ -509,72 +658,12 @@ struct TetArgs {
     const uint64_t *toff; // as-run fill: output offsets per ball
     uint32_t *tets_out;   // as-run fill: sorted-space vertex quadruples
     unsigned long long *ctr;
+    unsigned long long *gctr;  // the pass's counters (ctr may be a chunk's)
 };
 
 __device__ __forceinline__ void mark_face(uint64_t *F, uint64_t row_base, int W, int a, int b) {
     atomicOr((unsigned long long *)&F[row_base + (uint64_t)a * W + (b >> 6)],
              1ull << (b & 63));
-}
-
-// Empty-orthosphere test of one tetrahedron (checkTetsOrthosphere,
-// AlphaComplexLargeData.cu:606-734): 1 = some other ball violates,
-// 2 = none violates but some insphere value is exactly 0 (needs SoS),
-// 0 = empty.
-__device__ __forceinline__ int ortho_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
-                                          uint32_t v2, uint32_t v3, uint32_t v4,
-                                          const Ball a1, const Ball a2, const Ball a3,
-                                          const Ball a4, float4 sphere,
-                                          unsigned long long &evals,
-                                          unsigned long long &oob) {
-    float pa[3], pb[3], pc[3], pd[3], pe[3];
-    float wa, wb, wc, wd, we;
-    pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = a1.r * a1.r;
-    pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
-    pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
-    pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
-    int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
-    int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
-    int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
-    int currCellIndex = lin3(gridX, gridY, gridZ, G.gx, G.gy);
-    float orientation = pac::orient3d(pa, pb, pc, pd);
-    bool zero = false;
-    for (int q = 0; q < 27; q++) {
-        uint32_t beg, end;
-        if (q == 0) {
-            if (currCellIndex < 0 || (uint64_t)currCellIndex >= G.ncell) {
-                oob++;
-                continue;
-            }
-            uint64_t gc = G.cell_base + (uint64_t)currCellIndex;
-            beg = A.cellbeg[gc];
-            end = A.cellbeg[gc + 1];
-        } else {
-            int r = q - 1 + (q >= 14 ? 1 : 0);  // skip the centre (i = j = k = 0)
-            int i = r / 9 - 1, j = (r / 3) % 3 - 1, k = r % 3 - 1;
-            int zz = (int)((unsigned)gridZ + (unsigned)i), yy = (int)((unsigned)gridY + (unsigned)j),
-                xx = (int)((unsigned)gridX + (unsigned)k);
-            if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
-            if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
-            uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
-            beg = A.cellbeg[gc];
-            end = A.cellbeg[gc + 1];
-        }
-        for (uint32_t e = beg; e < end; e++) {
-            if (e == v1 || e == v2 || e == v3 || e == v4) continue;
-            const Ball atom = pac::ld_ball(&A.at[e]);
-            pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-            we = atom.r * atom.r;
-            evals++;
-            float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
-            if (orientation < 0) {
-                if (result < 0) return 1;
-            } else {
-                if (result > 0) return 1;
-            }
-            if (result == 0) zero = true;
-        }
-    }
-    return zero ? 2 : 0;
 }
 
 // One warp per ball v1.  For each upper neighbour v2 = N[a] the lanes take
@@ -583,15 +672,16 @@ __device__ __forceinline__ int ortho_test(const TetArgs &A, const MolGrid &G, ui
 // face (v2, v3, v4) is also an alpha triangle -- exactly the reference's
 // candidate tetrahedra (AlphaComplexLargeData.cu:350-529).  Each candidate
 // then passes markRealTets and, as written, the empty-orthosphere test.
-// MODE 0: as written, append survivors.  MODE 1: as run, count per ball.
-// MODE 2: as run, write in reference order (needs MODE 1 offsets).
+// As run (the orthosphere test skipped): MODE 1 counts per ball, MODE 2
+// writes in reference order (needs MODE 1's offsets).
 template <int V, int MODE>
 __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
     __shared__ uint16_t smap[8][kMaxDeg];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long cand_acc = 0, alpha_acc = 0, evals = 0, oob = 0;
+    unsigned long long cand_acc = 0, alpha_acc = 0;
+    Tally tally;
     for (uint64_t p = warp; p < A.n; p += nwarps) {
         const uint64_t e0 = A.eoff[p];
         const int deg = (int)(A.eoff[p + 1] - e0);
@@ -602,7 +692,6 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
             const uint64_t lp = A.loff[p];
             const uint64_t *Lp = A.link + lp;
             const Ball B1 = pac::ld_ball(&A.at[p]);
-            const MolGrid G = A.grids[mol_of(A.mol, p)];
             uint64_t out_base = (MODE == 2) ? A.toff[p] : 0;
             for (int a = 0; a < deg - 2; a++) {
                 uint64_t ra[kMaxW];
@@ -665,7 +754,7 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
                                     const uint32_t v4 = __ldg(&N[c]);
                                     const Ball B4 = pac::ld_ball(&A.at[v4]);
                                     float4 o;
-                                    if (!pac::tet_alpha(B1, B2, B3, B4, A.alpha, o)) continue;
+                                    if (!dec_tet<V>(B1, B2, B3, B4, A.alpha, o, tally)) continue;
                                     if (sweep == 1) alpha_acc++;
                                     if (MODE == 1) {
                                         lane_cnt++;
@@ -685,23 +774,6 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
                                         mark_face(A.faces, l2, W2, mb, mc);
                                         continue;
                                     }
-                                    int r = ortho_test(A, G, (uint32_t)p, v2, v3, v4, B1, B2, B3,
-                                                       B4, o, evals, oob);
-                                    if (r == 1) continue;
-                                    uint32_t key = (uint32_t)a | ((uint32_t)b << 8) |
-                                                   ((uint32_t)c << 16);
-                                    if (r == 2) {
-                                        unsigned long long q = atomicAdd(&A.ctr[C_PEND], 1ull);
-                                        if (q < A.pend_cap) A.pend[q] = make_uint2((uint32_t)p, key);
-                                        continue;
-                                    }
-                                    unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
-                                    if (q < A.surv_cap) A.surv[q] = make_uint2((uint32_t)p, key);
-                                    lane_cnt++;
-                                    mark_face(A.faces, lp, W, a, b);
-                                    mark_face(A.faces, lp, W, a, c);
-                                    mark_face(A.faces, lp, W, b, c);
-                                    mark_face(A.faces, l2, W2, mb, mc);
                                 }
                             }
                         }
@@ -719,29 +791,12 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
     }
     cand_acc = warp_sum(cand_acc);
     alpha_acc = warp_sum(alpha_acc);
-    evals = warp_sum(evals);
-    oob = warp_sum(oob);
+    if (MODE == 1) flush_tally<V>(tally, A.ctr);  // MODE 2 repeats MODE 1's tests
     if (lane == 0) {
         bump(A.ctr, C_CAND_Q, cand_acc);
         bump(A.ctr, C_ALPHA_Q, alpha_acc);
-        bump(A.ctr, C_INSPHERE, evals);
-        bump(A.ctr, C_OOB, oob);
     }
 }
-
-// As-written tetrahedra, one warp per ball v1, in three balanced phases:
-//  1. the candidate fourth vertices of every alpha triangle (v1, v2, v3) are
-//     flattened over the lanes (bits of rows a and b of v1's link matrix,
-//     checked against v2's link matrix), so each lane tests one candidate;
-//  2. each candidate gets markRealTets' alpha test, and the passing ones are
-//     queued in shared memory with their orthosphere's window cell;
-//  3. the queue is drained by work stealing: every lane owns one queued
-//     tetrahedron at a time and evaluates one window ball per step (the
-//     empty-orthosphere test of checkTetsOrthosphere), taking the next
-//     queued tetrahedron as soon as its own is decided.
-// The result does not depend on the order of the window balls: a
-// tetrahedron survives only if no ball violates its orthosphere.
-constexpr int kQCap = 192;
 
 __device__ __noinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
                                               const uint32_t *N, uint32_t key, bool pending,
@@ -773,12 +828,13 @@ constexpr int kSerialEvals = 8; // window balls a lane scans alone before handin
 // then the 26 neighbours range-checked per axis), a prefix sum over the cell
 // sizes flattens the window balls over the lanes.  Returns 1 = violated,
 // 2 = no violation but an exact zero, 0 = empty.
+template <int V>
 __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
                                          uint32_t v2, uint32_t v3, uint32_t v4, const float *pa,
                                          const float *pb, const float *pc, const float *pd,
                                          float wa, float wb, float wc, float wd,
                                          float orientation, int4 cl,
-                                         unsigned long long &evals) {
+                                         unsigned long long &evals, Tally &tally) {
     const int lane = threadIdx.x & 31;
     uint32_t beg = 0, cnt = 0;
     if (lane == 0) {
@@ -822,9 +878,9 @@ __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32
                 const Ball atom = pac::ld_ball(&A.at[x]);
                 float pe[3];
                 pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-                float we = atom.r * atom.r;
+                float we = wt<V>(atom.r);
                 evals++;
-                float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+                float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
                 viol = orientation < 0 ? (result < 0) : (result > 0);
                 if (result == 0) zero = true;
             }
@@ -832,280 +888,6 @@ __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32
         if (__any_sync(kFull, viol)) return 1;
     }
     return __any_sync(kFull, zero) ? 2 : 0;
-}
-
-template <int V>
-__global__ void __launch_bounds__(256, 2) k_tets_ws(TetArgs A) {
-    __shared__ uint16_t smap[8][kMaxDeg];
-    __shared__ uint32_t qkey[8][kQCap];
-    __shared__ int4 qcell[8][kQCap];
-    __shared__ uint32_t lkey[8][kLongCap];
-    __shared__ int4 lcell[8][kLongCap];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const unsigned lt_mask = (1u << lane) - 1;
-    unsigned long long cand_acc = 0, alpha_acc = 0, evals = 0, oob = 0;
-    while (true) {
-        uint64_t p = 0;
-        if (lane == 0) p = atomicAdd(&A.ctr[C_NEXT], 1ull);
-        p = __shfl_sync(kFull, p, 0);
-        if (p >= A.n) break;
-        const uint64_t e0 = A.eoff[p];
-        const int deg = (int)(A.eoff[p + 1] - e0);
-        uint32_t ball_count = 0;
-        if (deg >= 3) {
-            const int W = (deg + 63) >> 6;
-            const uint32_t *N = A.ER + e0;
-            const uint64_t lp = A.loff[p];
-            const uint64_t *Lp = A.link + lp;
-            const Ball B1 = pac::ld_ball(&A.at[p]);
-            const MolGrid G = A.grids[mol_of(A.mol, p)];
-            int qn = 0;
-
-            // phase 3: drain the queue (work stealing across the lanes)
-            auto drain = [&]() {
-                int head = 0;
-                bool have = false;
-                uint32_t key = 0;
-                float pa[3], pb[3], pc[3], pd[3], wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
-                uint32_t v2 = 0, v3 = 0, v4 = 0;
-                int gX = 0, gY = 0, gZ = 0, q = 0, nev = 0;
-                int4 mycell = make_int4(0, 0, 0, 0);
-                uint32_t e = 0, end = 0;
-                bool zero = false;
-                int ln = 0;  // long queue length (warp-uniform)
-                while (true) {
-                    unsigned want = __ballot_sync(kFull, !have);
-                    if (want && head < qn) {
-                        int r = __popc(want & lt_mask);
-                        if (!have && head + r < qn) {
-                            int idx = head + r;
-                            key = qkey[wib][idx];
-                            int4 cl = qcell[wib][idx];
-                            v2 = __ldg(&N[key & 0xff]);
-                            v3 = __ldg(&N[(key >> 8) & 0xff]);
-                            v4 = __ldg(&N[(key >> 16) & 0xff]);
-                            const Ball a2 = pac::ld_ball(&A.at[v2]), a3 = pac::ld_ball(&A.at[v3]),
-                                       a4 = pac::ld_ball(&A.at[v4]);
-                            pa[0] = B1.x, pa[1] = B1.y, pa[2] = B1.z, wa = B1.r * B1.r;
-                            pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
-                            pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
-                            pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
-                            orientation = pac::orient3d(pa, pb, pc, pd);
-                            gX = cl.x;
-                            gY = cl.y;
-                            gZ = cl.z;
-                            mycell = cl;
-                            int cc = cl.w;
-                            q = 0;
-                            nev = 0;
-                            zero = false;
-                            if (cc >= 0 && (uint64_t)cc < G.ncell) {
-                                uint64_t gc = G.cell_base + (uint64_t)cc;
-                                e = A.cellbeg[gc];
-                                end = A.cellbeg[gc + 1];
-                            } else {
-                                e = end = 0;
-                                oob++;
-                            }
-                            have = true;
-                        }
-                        head = min(qn, head + __popc(want));
-                    }
-                    if (!__any_sync(kFull, have)) break;
-                    // a tetrahedron still open after kSerialEvals balls goes to
-                    // the cooperative scan, so no lane runs a long window alone
-                    const bool handoff = have && nev >= kSerialEvals;
-                    const unsigned hm = __ballot_sync(kFull, handoff);
-                    if (hm) {
-                        int pos = ln + __popc(hm & lt_mask);
-                        if (handoff && pos < kLongCap) {
-                            lkey[wib][pos] = key;
-                            lcell[wib][pos] = mycell;
-                            have = false;
-                        }
-                        ln = min(kLongCap, ln + __popc(hm));
-                    }
-                    if (!have) continue;
-                    if (e < end) {
-                        uint32_t x = e++;
-                        if (x == (uint32_t)p || x == v2 || x == v3 || x == v4) continue;
-                        const Ball atom = pac::ld_ball(&A.at[x]);
-                        float pe[3];
-                        pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-                        float we = atom.r * atom.r;
-                        evals++;
-                        nev++;
-                        float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
-                        bool viol = orientation < 0 ? (result < 0) : (result > 0);
-                        if (viol) {
-                            have = false;
-                            continue;
-                        }
-                        if (result == 0) zero = true;
-                        continue;
-                    }
-                    // next window cell: the 26 neighbours of the centre cell,
-                    // range-checked per axis (AlphaComplexLargeData.cu:673-685)
-                    bool found = false;
-                    while (q < 26 && !found) {
-                        q++;
-                        int rr = q - 1 + (q >= 14 ? 1 : 0);
-                        int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
-                        int zz = (int)((unsigned)gZ + (unsigned)i),
-                            yy = (int)((unsigned)gY + (unsigned)j),
-                            xx = (int)((unsigned)gX + (unsigned)k);
-                        if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
-                        if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
-                        uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
-                        e = A.cellbeg[gc];
-                        end = A.cellbeg[gc + 1];
-                        found = true;
-                    }
-                    if (!found) {
-                        emit_survivor(A, p, W, lp, N, key, zero, ball_count);
-                        have = false;
-                    }
-                }
-                __syncwarp();
-                for (int t = 0; t < ln; t++) {
-                    const uint32_t k2 = lkey[wib][t];
-                    const int4 cl = lcell[wib][t];
-                    const uint32_t u2 = __ldg(&N[k2 & 0xff]), u3 = __ldg(&N[(k2 >> 8) & 0xff]),
-                                   u4 = __ldg(&N[(k2 >> 16) & 0xff]);
-                    const Ball a2 = pac::ld_ball(&A.at[u2]), a3 = pac::ld_ball(&A.at[u3]),
-                               a4 = pac::ld_ball(&A.at[u4]);
-                    float qa[3], qb[3], qc[3], qd[3];
-                    qa[0] = B1.x, qa[1] = B1.y, qa[2] = B1.z;
-                    qb[0] = a2.x, qb[1] = a2.y, qb[2] = a2.z;
-                    qc[0] = a3.x, qc[1] = a3.y, qc[2] = a3.z;
-                    qd[0] = a4.x, qd[1] = a4.y, qd[2] = a4.z;
-                    const float xa = B1.r * B1.r, xb = a2.r * a2.r, xc = a3.r * a3.r,
-                                xd = a4.r * a4.r;
-                    const float ori = pac::orient3d(qa, qb, qc, qd);
-                    int r = coop_test(A, G, (uint32_t)p, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc,
-                                      xd, ori, cl, evals);
-                    if (r != 1 && lane == 0) emit_survivor(A, p, W, lp, N, k2, r == 2, ball_count);
-                }
-                __syncwarp();
-            };
-
-            for (int a = 0; a < deg - 2; a++) {
-                uint64_t ra[kMaxW];
-                int nb = 0;
-#pragma unroll
-                for (int w = 0; w < kMaxW; w++) {
-                    ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
-                    nb += __popcll(ra[w]);
-                }
-                if (nb < 2) continue;
-                const uint32_t v2 = __ldg(&N[a]);
-                const uint64_t e2 = A.eoff[v2];
-                const int deg2 = (int)(A.eoff[v2 + 1] - e2);
-                const int W2 = (deg2 + 63) >> 6;
-                const uint64_t *L2 = A.link + A.loff[v2];
-                for (int c = a + 1 + lane; c < deg; c += 32) {
-                    uint32_t x = __ldg(&N[c]);
-                    int pos = lbound(A.ER + e2, deg2, x);
-                    smap[wib][c] = (pos < deg2 && __ldg(&A.ER[e2 + pos]) == x) ? (uint16_t)pos
-                                                                               : (uint16_t)0xffff;
-                }
-                __syncwarp();
-                const Ball B2 = pac::ld_ball(&A.at[v2]);
-                for (int k0 = 0; k0 < nb; k0 += 32) {
-                    // phase 1: this lane's alpha triangle (v1, v2, N[b]) and its
-                    // candidate fourth vertices
-                    int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
-                    uint64_t m[kMaxW];
-                    int cnt = 0;
-#pragma unroll
-                    for (int w = 0; w < kMaxW; w++) {
-                        m[w] = (b >= 0 && w < W) ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
-                                                 : 0;
-                        cnt += __popcll(m[w]);
-                    }
-                    int incl = cnt;
-                    for (int o = 1; o < 32; o <<= 1) {
-                        int v = __shfl_up_sync(kFull, incl, o);
-                        if (lane >= o) incl += v;
-                    }
-                    const int total = __shfl_sync(kFull, incl, 31);
-                    for (int base = 0; base < total; base += 32) {
-                        const int s = base + lane;
-                        int lo = 0;
-                        for (int step = 16; step; step >>= 1) {
-                            int v = __shfl_sync(kFull, incl, lo + step - 1);
-                            if (v <= s) lo += step;
-                        }
-                        const int owner = lo & 31;
-                        const int oincl = __shfl_sync(kFull, incl, owner);
-                        const int ocnt = __shfl_sync(kFull, cnt, owner);
-                        const int bo = __shfl_sync(kFull, b, owner);
-                        uint64_t mo[kMaxW];
-#pragma unroll
-                        for (int w = 0; w < kMaxW; w++) {
-                            uint32_t lo32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
-                            uint32_t hi32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
-                            mo[w] = ((uint64_t)hi32 << 32) | lo32;
-                        }
-                        bool pass4 = false, passA = false;
-                        int c = -1;
-                        int4 cell = make_int4(0, 0, 0, 0);
-                        if (s < total) {
-                            c = select_bit(mo, W, s - (oincl - ocnt));
-                            const int mb = smap[wib][bo], mc = smap[wib][c];
-                            pass4 = mb != 0xffff && mc != 0xffff &&
-                                    ((__ldg(&L2[(uint64_t)mb * W2 + (mc >> 6)]) >> (mc & 63)) & 1ull);
-                            if (pass4) {
-                                const Ball B3 = pac::ld_ball(&A.at[__ldg(&N[bo])]);
-                                const Ball B4 = pac::ld_ball(&A.at[__ldg(&N[c])]);
-                                float4 sphere;
-                                passA = pac::tet_alpha(B1, B2, B3, B4, A.alpha, sphere);
-                                if (passA) {
-                                    int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
-                                    int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
-                                    int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
-                                    cell = make_int4(gridX, gridY, gridZ,
-                                                     lin3(gridX, gridY, gridZ, G.gx, G.gy));
-                                }
-                            }
-                        }
-                        const unsigned m4 = __ballot_sync(kFull, pass4);
-                        const unsigned mA = __ballot_sync(kFull, passA);
-                        if (passA) {
-                            int pos = qn + __popc(mA & lt_mask);
-                            qkey[wib][pos] = (uint32_t)a | ((uint32_t)bo << 8) | ((uint32_t)c << 16);
-                            qcell[wib][pos] = cell;
-                        }
-                        qn += __popc(mA);
-                        cand_acc += lane == 0 ? __popc(m4) : 0;
-                        alpha_acc += lane == 0 ? __popc(mA) : 0;
-                        __syncwarp();
-                        if (qn > kQCap - 32) {
-                            drain();
-                            qn = 0;
-                        }
-                    }
-                }
-                __syncwarp();
-            }
-            if (qn) drain();
-        }
-        {
-            uint32_t s = ball_count;
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-            if (lane == 0) A.tcount[p] = s;
-        }
-    }
-    cand_acc = warp_sum(cand_acc);
-    alpha_acc = warp_sum(alpha_acc);
-    evals = warp_sum(evals);
-    oob = warp_sum(oob);
-    if (lane == 0) {
-        bump(A.ctr, C_CAND_Q, cand_acc);
-        bump(A.ctr, C_ALPHA_Q, alpha_acc);
-        bump(A.ctr, C_INSPHERE, evals);
-        bump(A.ctr, C_OOB, oob);
-    }
 }
 
 // ---- the as-written tetrahedra in two kernels over an HBM queue ----------
@@ -1129,6 +911,7 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
     unsigned long long cand_acc = 0, alpha_acc = 0;
+    Tally tally;
     while (true) {
         uint64_t p = 0;
         if (lane == 0) {
@@ -1216,7 +999,7 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
                             const Ball B3 = pac::ld_ball(&A.at[__ldg(&N[bo])]);
                             const Ball B4 = pac::ld_ball(&A.at[__ldg(&N[c])]);
                             float4 sphere;
-                            passA = pac::tet_alpha(B1, B2, B3, B4, A.alpha, sphere);
+                            passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
                             if (passA) {
                                 int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
                                 int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
@@ -1248,6 +1031,7 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
             __syncwarp();
         }
     }
+    flush_tally<V>(tally, A.gctr);
     if (lane == 0) {
         bump(A.ctr, C_CAND_Q, cand_acc);
         bump(A.ctr, C_ALPHA_Q, alpha_acc);
@@ -1262,6 +1046,7 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
 // kSerialEvals balls is handed to the cooperative test (the whole warp scans
 // its window), so no lane runs a long window alone.  Survivors are recorded
 // and mark their faces.
+template <int V>
 __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
     __shared__ uint32_t lkey[8][kLongCap];
@@ -1270,6 +1055,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
     unsigned long long evals = 0, oob = 0;
+    Tally tally;
     uint64_t head = 0, tail = 0;  // this warp's claimed range (warp-uniform)
     bool have = false, more = true;
     uint32_t p = 0, key = 0, v2 = 0, v3 = 0, v4 = 0;
@@ -1294,10 +1080,11 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             qb[0] = a2.x, qb[1] = a2.y, qb[2] = a2.z;
             qc[0] = a3.x, qc[1] = a3.y, qc[2] = a3.z;
             qd[0] = a4.x, qd[1] = a4.y, qd[2] = a4.z;
-            const float xa = a1.r * a1.r, xb = a2.r * a2.r, xc = a3.r * a3.r, xd = a4.r * a4.r;
-            const float ori = pac::orient3d(qa, qb, qc, qd);
+            const float xa = wt<V>(a1.r), xb = wt<V>(a2.r), xc = wt<V>(a3.r), xd = wt<V>(a4.r);
+            const float ori = dec_orient<V>(qa, qb, qc, qd, xa, xb, xc, xd, tally);
             const MolGrid G2 = A.grids[mol_of(A.mol, p2)];
-            int r = coop_test(A, G2, p2, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc, xd, ori, cl, evals);
+            int r = coop_test<V>(A, G2, p2, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc, xd, ori, cl, evals,
+                                 tally);
             if (r != 1 && lane == 0) {
                 const int deg = (int)(A.eoff[p2 + 1] - A.eoff[p2]);
                 uint32_t dummy = 0;
@@ -1334,11 +1121,11 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
                 v4 = __ldg(&N[(key >> 16) & 0xff]);
                 const Ball a1 = pac::ld_ball(&A.at[p]), a2 = pac::ld_ball(&A.at[v2]),
                            a3 = pac::ld_ball(&A.at[v3]), a4 = pac::ld_ball(&A.at[v4]);
-                pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = a1.r * a1.r;
-                pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = a2.r * a2.r;
-                pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = a3.r * a3.r;
-                pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = a4.r * a4.r;
-                orientation = pac::orient3d(pa, pb, pc, pd);
+                pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = wt<V>(a1.r);
+                pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = wt<V>(a2.r);
+                pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = wt<V>(a3.r);
+                pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = wt<V>(a4.r);
+                orientation = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
                 gX = cl.x;
                 gY = cl.y;
                 gZ = cl.z;
@@ -1388,10 +1175,10 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             const Ball atom = pac::ld_ball(&A.at[x]);
             float pe[3];
             pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-            float we = atom.r * atom.r;
+            float we = wt<V>(atom.r);
             evals++;
             nev++;
-            float result = pac::insphere_w(pa, pb, pc, pd, pe, wa, wb, wc, wd, we);
+            float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
             bool viol = orientation < 0 ? (result < 0) : (result > 0);
             if (viol) {
                 have = false;
@@ -1426,6 +1213,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
     }
     evals = warp_sum(evals);
     oob = warp_sum(oob);
+    flush_tally<V>(tally, A.ctr);
     if (lane == 0) {
         bump(A.ctr, C_INSPHERE, evals);
         bump(A.ctr, C_OOB, oob);
@@ -1435,6 +1223,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
 // Tetrahedra whose window holds an insphere value of exactly 0: the test
 // again, with the reference's simulation of simplicity for those balls
 // (AlphaComplexLargeData.cu:645-652, 659-667).
+template <int V>
 __global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npend) return;
@@ -1448,8 +1237,9 @@ __global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
     uint32_t v[4] = {(uint32_t)p, N[a], N[b], N[c]};
     Ball B[4];
     for (int k = 0; k < 4; k++) B[k] = pac::ld_ball(&A.at[v[k]]);
+    Tally tally;
     float4 sphere;
-    pac::tet_alpha(B[0], B[1], B[2], B[3], A.alpha, sphere);
+    dec_tet<V>(B[0], B[1], B[2], B[3], A.alpha, sphere, tally);
     const MolGrid G = A.grids[mol_of(A.mol, p)];
     float pts[5][3], ws[5];
     int idx[5];
@@ -1457,10 +1247,11 @@ __global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
         pts[k][0] = B[k].x;
         pts[k][1] = B[k].y;
         pts[k][2] = B[k].z;
-        ws[k] = B[k].r * B[k].r;
+        ws[k] = wt<V>(B[k].r);
         idx[k] = (int)A.orig[v[k]] + 1;
     }
-    float orientation = pac::orient3d(pts[0], pts[1], pts[2], pts[3]);
+    float orientation = dec_orient<V>(pts[0], pts[1], pts[2], pts[3], ws[0], ws[1], ws[2], ws[3],
+                                      tally);
     int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
     int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
     int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
@@ -1489,19 +1280,20 @@ __global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
             pts[4][0] = atom.x;
             pts[4][1] = atom.y;
             pts[4][2] = atom.z;
-            ws[4] = atom.r * atom.r;
-            float result = pac::insphere_w(pts[0], pts[1], pts[2], pts[3], pts[4], ws[0], ws[1],
-                                           ws[2], ws[3], ws[4]);
+            ws[4] = wt<V>(atom.r);
+            float result = dec_insphere<V>(pts[0], pts[1], pts[2], pts[3], pts[4], ws[0], ws[1],
+                                           ws[2], ws[3], ws[4], tally);
             if (result == 0) {
                 idx[4] = (int)A.orig[e] + 1;
                 int status = 0;
-                result = (float)pac::sos_orientation(pts, ws, idx, &status);
+                result = (float)pac::sos_orientation(pts, ws, idx, &status, V == pac::kExact);
                 atomicAdd(&A.ctr[C_SOS], 1ull);
                 if (status == 1) atomicAdd(&A.ctr[C_SOS_RANGE], 1ull);
             }
             viol = orientation < 0 ? (result < 0) : (result > 0);
         }
     }
+    flush_tally_thread<V>(tally, A.ctr);
     if (viol) return;
     unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
     if (q < A.surv_cap) A.surv[q] = pk;
@@ -1562,133 +1354,10 @@ __global__ void k_map4(uint64_t nq, const uint32_t *orig, uint32_t *tets) {
 }
 
 // ------------------------------------------------------------------ attachment
-// Final triangles of ball i: tetrahedron faces, plus the alpha triangles
+// Final triangles of ball v1: tetrahedron faces, plus the alpha triangles
 // that are not faces and whose orthosphere no other ball of the 27-cell
 // window reaches (checkDanglingTris, AlphaComplexLargeData.cu:798-872).
-// Also marks the three edges of every final triangle.
-template <int V>
-__global__ void __launch_bounds__(256) k_tri_final(uint64_t n, const float4 *__restrict__ at,
-                                                   const uint64_t *__restrict__ eoff,
-                                                   const uint32_t *__restrict__ ER,
-                                                   const uint64_t *__restrict__ loff,
-                                                   const uint64_t *__restrict__ link,
-                                                   uint64_t *faces, uint32_t *tricount,
-                                                   uint8_t *eflag, const uint32_t *cellbeg,
-                                                   const uint32_t *mol, const MolGrid *grids,
-                                                   float alpha, unsigned long long *ctr) {
-    __shared__ uint64_t sfin[8][kMaxW];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long oob = 0;
-    for (uint64_t p = warp; p < n; p += nwarps) {
-        const uint64_t e0 = eoff[p];
-        const int deg = (int)(eoff[p + 1] - e0);
-        uint32_t count = 0;
-        if (deg >= 2) {
-            const int W = (deg + 63) >> 6;
-            const uint32_t *N = ER + e0;
-            const uint64_t lp = loff[p];
-            const Ball A0 = pac::ld_ball(&at[p]);
-            const MolGrid G = grids[mol_of(mol, p)];
-            for (int a = 0; a < deg - 1; a++) {
-                uint64_t la[kMaxW], fa[kMaxW], cand[kMaxW];
-                int nc = 0;
-#pragma unroll
-                for (int w = 0; w < kMaxW; w++) {
-                    la[w] = w < W ? link[lp + (uint64_t)a * W + w] : 0;
-                    fa[w] = w < W ? faces[lp + (uint64_t)a * W + w] : 0;
-                    cand[w] = la[w] & ~fa[w];
-                    nc += __popcll(cand[w]);
-                }
-                if (!__any_sync(kFull, (la[0] | la[1] | la[2] | la[3]) != 0)) continue;
-                if (lane < kMaxW) sfin[wib][lane] = lane < W ? faces[lp + (uint64_t)a * W + lane] : 0;
-                __syncwarp();
-                const uint32_t v1 = N[a];
-                const Ball A1 = pac::ld_ball(&at[v1]);
-                for (int k0 = 0; k0 < nc; k0 += 32) {
-                    int b = (k0 + lane < nc) ? select_bit(cand, W, k0 + lane) : -1;
-                    bool keep = false;
-                    if (b >= 0) {
-                        const uint32_t v2 = N[b];
-                        float4 p1;
-                        pac::tri_alpha<V>(A0, A1, pac::ld_ball(&at[v2]), alpha, p1);
-                        float currentDist = p1.w;
-                        int gridX = pac::cell_coord(p1.x, G.minx, G.step);
-                        int gridY = pac::cell_coord(p1.y, G.miny, G.step);
-                        int gridZ = pac::cell_coord(p1.z, G.minz, G.step);
-                        int cc = lin3(gridX, gridY, gridZ, G.gx, G.gy);
-                        bool att = false;
-                        for (int q = 0; q < 27 && !att; q++) {
-                            uint32_t beg, end;
-                            if (q == 0) {
-                                if (cc < 0 || (uint64_t)cc >= G.ncell) {
-                                    oob++;
-                                    continue;
-                                }
-                                beg = cellbeg[G.cell_base + cc];
-                                end = cellbeg[G.cell_base + cc + 1];
-                            } else {
-                                int r = q - 1 + (q >= 14 ? 1 : 0);
-                                int i = r / 9 - 1, j = (r / 3) % 3 - 1, k = r % 3 - 1;
-                                int zz = (int)((unsigned)gridZ + (unsigned)i),
-                                    yy = (int)((unsigned)gridY + (unsigned)j),
-                                    xx = (int)((unsigned)gridX + (unsigned)k);
-                                if ((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) continue;
-                                if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
-                                uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
-                                beg = cellbeg[gc];
-                                end = cellbeg[gc + 1];
-                            }
-                            for (uint32_t e = beg; e < end; e++) {
-                                if (e == p || e == v1 || e == v2) continue;
-                                if (pac::attached(pac::ld_ball(&at[e]), p1.x, p1.y, p1.z,
-                                                  currentDist)) {
-                                    att = true;
-                                    break;
-                                }
-                            }
-                        }
-                        keep = !att;
-                    }
-                    if (keep) atomicOr((unsigned long long *)&sfin[wib][b >> 6], 1ull << (b & 63));
-                }
-                __syncwarp();
-                // final row: write, count, and mark the edges of its triangles
-                uint64_t fin[kMaxW];
-                int nf = 0;
-#pragma unroll
-                for (int w = 0; w < kMaxW; w++) {
-                    fin[w] = sfin[wib][w];
-                    nf += __popcll(fin[w]);
-                }
-                __syncwarp();
-                if (lane < W) faces[lp + (uint64_t)a * W + lane] = fin[lane];
-                count += nf;
-                if (nf) {
-                    if (lane == 0) eflag[e0 + a] = 1;
-                    const uint64_t e1 = eoff[v1];
-                    const int deg1 = (int)(eoff[v1 + 1] - e1);
-                    for (int k0 = 0; k0 < nf; k0 += 32) {
-                        int b = (k0 + lane < nf) ? select_bit(fin, W, k0 + lane) : -1;
-                        if (b >= 0) {
-                            eflag[e0 + b] = 1;
-                            const uint32_t v2 = N[b];
-                            int pos = lbound(ER + e1, deg1, v2);
-                            if (pos < deg1 && ER[e1 + pos] == v2) eflag[e1 + pos] = 1;
-                        }
-                    }
-                }
-            }
-        }
-        if (lane == 0) tricount[p] = count;
-    }
-    oob = warp_sum(oob);
-    if (lane == 0) bump(ctr, C_OOB, oob);
-}
-
-// Final triangles with work stealing (same decisions as k_tri_final): one
-// warp per ball v1, balls handed out from a counter.  The alpha triangles
+// Work stealing: one warp per ball v1, balls handed out from a counter.  The alpha triangles
 // of v1 that are not tetrahedron faces are queued in shared memory row by
 // row; each lane takes one, recomputes its orthosphere (markRealTriangles)
 // and tests one window ball per step (checkDanglingTris,
@@ -1711,6 +1380,7 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
     unsigned long long oob = 0;
+    Tally tally;
     while (true) {
         uint64_t p = 0;
         if (lane == 0) p = atomicAdd(&ctr[C_NEXT], 1ull);
@@ -1783,9 +1453,8 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
                         tb = qb[wib][head + r];
                         v1 = N[ta];
                         v2 = N[tb];
-                        float4 p1;
-                        pac::tri_alpha<V>(A0, pac::ld_ball(&at[v1]), pac::ld_ball(&at[v2]), alpha,
-                                          p1);
+                        const float4 p1 =
+                            tri_sphere<V>(A0, pac::ld_ball(&at[v1]), pac::ld_ball(&at[v2]), alpha);
                         px = p1.x;
                         py = p1.y;
                         pz = p1.z;
@@ -1814,7 +1483,9 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
                 if (e < end) {
                     uint32_t x = e++;
                     if (x == (uint32_t)p || x == v1 || x == v2) continue;
-                    if (pac::attached(pac::ld_ball(&at[x]), px, py, pz, cur)) have = false;
+                    if (dec_tri_attached<V>(A0, at, v1, v2, pac::ld_ball(&at[x]), px, py, pz, cur,
+                                            tally))
+                        have = false;
                     continue;
                 }
                 bool found = false;
@@ -1869,6 +1540,7 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
         if (lane == 0) tricount[p] = count;
     }
     oob = warp_sum(oob);
+    flush_tally<V>(tally, ctr);
     if (lane == 0) bump(ctr, C_OOB, oob);
 }
 
@@ -1885,6 +1557,7 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long oob = 0;
+    Tally tally;
     for (uint64_t p = warp; p < n; p += nwarps) {
         const uint64_t e0 = eoff[p];
         const int deg = (int)(eoff[p + 1] - e0);
@@ -1895,7 +1568,8 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__
             if (eflag[e0 + k]) continue;
             const uint32_t v2 = ER[e0 + k];
             float px, py, pz, currentDist;
-            pac::edge_foot(a1, pac::ld_ball(&at[v2]), px, py, pz, currentDist);
+            const Ball a2 = pac::ld_ball(&at[v2]);
+            edge_sphere<V>(a1, a2, px, py, pz, currentDist);
             int gridX = pac::cell_coord(px, G.minx, G.step);
             int gridY = pac::cell_coord(py, G.miny, G.step);
             int gridZ = pac::cell_coord(pz, G.minz, G.step);
@@ -1924,7 +1598,8 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__
                 }
                 for (uint32_t e = beg; e < end; e++) {
                     if (e == p || e == v2) continue;
-                    if (pac::attached(pac::ld_ball(&at[e]), px, py, pz, currentDist)) {
+                    if (dec_edge_attached<V>(a1, a2, pac::ld_ball(&at[e]), px, py, pz,
+                                             currentDist, tally)) {
                         att = true;
                         break;
                     }
@@ -1934,6 +1609,7 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__
         }
     }
     oob = warp_sum(oob);
+    flush_tally<V>(tally, ctr);
     if (lane == 0) bump(ctr, C_OOB, oob);
 }
 
@@ -2161,6 +1837,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     T.grids = grids;
     T.alpha = in.alpha;
     T.ctr = ctr;
+    T.gctr = ctr;
     T.tcount = ar.alloc_n<uint32_t>(n);
     uint64_t *toff = ar.alloc_n<uint64_t>(n + 1);
     if (!T.tcount || !toff) return PAC_ERR_OOM;
@@ -2247,7 +1924,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             cand_total += ha[C_CAND_Q];
             alpha_total += ha[C_ALPHA_Q];
             CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
-            k_tets_scan<<<148 * 4, 256, 0, s>>>(T, Q, queued, claim);
+            k_tets_scan<V><<<148 * 4, 256, 0, s>>>(T, Q, queued, claim);
             LAUNCH_CHECK(ctx);
             // next chunk sized from this one's queue fill
             if (queued)
@@ -2275,7 +1952,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             T.surv_cap = sp[0] + sp[1];
         }
         if (sp[1]) {
-            k_sos_resolve<<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
+            k_sos_resolve<V><<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
             LAUNCH_CHECK(ctx);
             CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
@@ -2380,6 +2057,8 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         st->final_tets = nQ;
         st->insphere_evals = hc[C_INSPHERE];
         st->sos_calls = hc[C_SOS];
+        st->filter_evals = hc[C_FILTER];
+        st->exact_fallbacks = hc[C_FALLBACK];
         st->ortho_out_of_grid = hc[C_OOB];
         st->max_degree = maxdeg;
         st->ms_grid = tm.ms(0, 1);
@@ -2401,6 +2080,13 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
 
 int run_pass(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::PassInput &in,
              pac::PassOutput &out, pac_stats *st) {
+    if (cfg.exact) {
+#if PAC_WITH_EXACT
+        return run_pass_v<pac::kExact>(ctx, cfg, in, out, st);
+#else
+        return pac::set_error(PAC_ERR_INVALID_ARG, "exact predicates are built in the strict flavour");
+#endif
+    }
     if (cfg.formula == PAC_FORMULA_PLAIN_XMP) return run_pass_v<pac::kPlainXmp>(ctx, cfg, in, out, st);
     return run_pass_v<pac::kUpstream>(ctx, cfg, in, out, st);
 }

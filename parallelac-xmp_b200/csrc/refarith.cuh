@@ -27,7 +27,8 @@ __device__ __forceinline__ Ball ld_ball(const float4 *p) {
     return Ball{v.x, v.y, v.z, v.w};
 }
 
-enum : int { kUpstream = 0, kPlainXmp = 1 };
+// formula sets; kExact selects the decision-exact predicates (exactpred.cuh)
+enum : int { kUpstream = 0, kPlainXmp = 1, kExact = 2 };
 
 // markRealEdges: LD:173-189 (upstream) / PLAIN:209-229 (plain-xmp).
 template <int V>

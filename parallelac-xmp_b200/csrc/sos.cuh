@@ -229,9 +229,11 @@ static __device__ __noinline__ int sos_minor(const SosPoints &s, int depth) {
 // Sign of orientation4SoS_w(p[0..4], w[0..4], idx[0..4]).  Returns +1/-1;
 // *status is 0, or 1 when the input range exceeds the integer width, or 2
 // when every minor vanishes (the reference does not terminate there; this
-// returns +1, the value its last depth is meant to give).
+// returns +1, the value its last depth is meant to give).  With radii set,
+// w[] holds radii and the weights are their exact squares (the
+// decision-exact mode); otherwise w[] holds the binary32 weights.
 static __device__ __noinline__ int sos_orientation(const float (*p)[3], const float *w,
-                                            const int *index, int *status) {
+                                            const int *index, int *status, bool radii = false) {
     int idx[5], ord[5];
     for (int i = 0; i < 5; i++) { idx[i] = index[i]; ord[i] = i; }
     int swaps = 0;
@@ -263,7 +265,13 @@ static __device__ __noinline__ int sos_orientation(const float (*p)[3], const fl
             bi_mul(sq, s.c[i][k], s.c[i][k]);
             bi_add(acc, acc, sq);
         }
-        bi_from_float(s.w[i], w[ord[i]], 2 * emin);
+        if (radii) {
+            BigInt r;
+            bi_from_float(r, w[ord[i]], emin);
+            bi_mul(s.w[i], r, r);
+        } else {
+            bi_from_float(s.w[i], w[ord[i]], 2 * emin);
+        }
         bi_sub(s.lift[i], acc, s.w[i]);
     }
     int sign = 0, depth = 0;
