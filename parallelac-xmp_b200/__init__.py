@@ -403,3 +403,47 @@ def batch(sizes, seed=SEED_BASE + 3):
     if _synth().pac_synth_batch(seed, len(sizes), sizes.ctypes.data, out.ctypes.data) != 0:
         raise MemoryError("generator allocation failed")
     return out, off
+
+
+# ---------------------------------------------------------------- many GPUs
+def shard_molecules(sizes, world):
+    """Greedy size balance of independent molecules over `world` ranks:
+    largest first, each to the least-loaded rank (ties to the lower rank).
+    Returns one ascending index array per rank."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for m in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(m)
+        load[r] += int(sizes[m])
+    return [np.array(sorted(p), dtype=np.int64) for p in parts]
+
+
+def sharded_batch(balls, offsets, rank, world, run, group=None):
+    """Many molecules over the ranks of a torch.distributed group: rank r
+    computes the molecules shard_molecules() gives it with
+    run(balls, offsets) -> [(edges, tris, tets)] (one rank-local batched
+    pass, e.g. an Engine's alpha_complex_batch), and rank 0 receives every
+    molecule's lists in the original order (None on the other ranks).  The
+    molecules are independent: the only collective is this final gather."""
+    import torch.distributed as dist
+    off = np.asarray(offsets, dtype=np.uint64)
+    sizes = np.diff(off.astype(np.int64))
+    mine = shard_molecules(sizes, world)[rank]
+    if len(mine):
+        parts = [np.asarray(balls[off[m]:off[m + 1]]) for m in mine]
+        loff = np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint64)
+        res = run(np.concatenate(parts), loff)
+    else:
+        res = []
+    local = [(int(m), tuple(np.asarray(x) for x in r)) for m, r in zip(mine, res)]
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object(local, gathered, dst=0, group=group)
+    if rank != 0:
+        return None
+    out = [None] * len(sizes)
+    for part in gathered:
+        for m, r in part:
+            out[m] = r
+    return out

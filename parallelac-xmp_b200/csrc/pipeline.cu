@@ -1169,23 +1169,48 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             }
         }
         if (!have) continue;
-        if (e < end) {
-            uint32_t x = e++;
-            if (x == p || x == v2 || x == v3 || x == v4) continue;
-            const Ball atom = pac::ld_ball(&A.at[x]);
-            float pe[3];
-            pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-            float we = wt<V>(atom.r);
-            evals++;
-            nev++;
-            float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
-            bool viol = orientation < 0 ? (result < 0) : (result > 0);
-            if (viol) {
-                have = false;
+        if constexpr (V != pac::kExact) {
+            // two window balls per step: independent loads and arithmetic
+            // overlap, and the warp-wide bookkeeping above runs half as often
+            if (e < end) {
+                const uint32_t x0 = e, x1 = (e + 1 < end) ? e + 1 : e;
+                const bool ok0 = !(x0 == p || x0 == v2 || x0 == v3 || x0 == v4);
+                const bool ok1 = x1 != x0 && !(x1 == p || x1 == v2 || x1 == v3 || x1 == v4);
+                e = x1 + 1;
+                const Ball b0 = pac::ld_ball(&A.at[x0]), b1 = pac::ld_ball(&A.at[x1]);
+                float pe0[3] = {b0.x, b0.y, b0.z}, pe1[3] = {b1.x, b1.y, b1.z};
+                const float r0 = dec_insphere<V>(pa, pb, pc, pd, pe0, wa, wb, wc, wd, wt<V>(b0.r), tally);
+                const float r1 = dec_insphere<V>(pa, pb, pc, pd, pe1, wa, wb, wc, wd, wt<V>(b1.r), tally);
+                evals += (int)ok0 + (int)ok1;
+                nev += (int)ok0 + (int)ok1;
+                const bool viol = (ok0 && (orientation < 0 ? (r0 < 0) : (r0 > 0))) ||
+                                  (ok1 && (orientation < 0 ? (r1 < 0) : (r1 > 0)));
+                if (viol) {
+                    have = false;
+                    continue;
+                }
+                if ((ok0 && r0 == 0) || (ok1 && r1 == 0)) zero = true;
                 continue;
             }
-            if (result == 0) zero = true;
-            continue;
+        } else {
+            if (e < end) {
+                uint32_t x = e++;
+                if (x == p || x == v2 || x == v3 || x == v4) continue;
+                const Ball atom = pac::ld_ball(&A.at[x]);
+                float pe[3];
+                pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
+                float we = wt<V>(atom.r);
+                evals++;
+                nev++;
+                float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
+                bool viol = orientation < 0 ? (result < 0) : (result > 0);
+                if (viol) {
+                    have = false;
+                    continue;
+                }
+                if (result == 0) zero = true;
+                continue;
+            }
         }
         bool found = false;
         const int Ggx = G->gx, Ggy = G->gy, Ggz = G->gz;
