@@ -77,6 +77,7 @@ class Stats(ctypes.Structure):
     def as_dict(self):
         d = {k: int(getattr(self, k)) for k in _STAT_U64}
         d.update({k: float(getattr(self, k)) for k in _STAT_F64})
+        d["bytes_model"] = int(self.bytes_model)
         d["grid"] = list(self.grid)
         d["step"] = float(self.step)
         d["kernels_launched"] = int(self.kernels_launched)

@@ -7,7 +7,7 @@
 // Same argument checks, exit codes, stdout report and output file.  Two
 // environment variables choose what the positional interface cannot:
 //   PAC_TET_MODE   = as-run (default: the reference binary's output) | as-written
-//   PAC_PREDICATES = strict (default) | fma
+//   PAC_PREDICATES = strict (default) | fma | exact
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -56,7 +56,9 @@ int main(int argc, char **argv) {
     const char *tm = std::getenv("PAC_TET_MODE");
     opt.tet_mode = (tm && std::strcmp(tm, "as-written") == 0) ? PAC_TETS_AS_WRITTEN : PAC_TETS_AS_RUN;
     const char *pm = std::getenv("PAC_PREDICATES");
-    opt.predicates = (pm && std::strcmp(pm, "fma") == 0) ? PAC_PRED_REFCOMPAT_FMA : PAC_PRED_REFCOMPAT;
+    opt.predicates = (pm && std::strcmp(pm, "fma") == 0)     ? PAC_PRED_REFCOMPAT_FMA
+                     : (pm && std::strcmp(pm, "exact") == 0) ? PAC_PRED_EXACT
+                                                             : PAC_PRED_REFCOMPAT;
     pac_ctx *ctx = nullptr;
     rc = pac_create(&ctx, &opt);
     pac_complex cx;

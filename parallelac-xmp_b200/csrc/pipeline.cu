@@ -2093,6 +2093,13 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         st->ms_tri_attach = tm.ms(4, 5);
         st->ms_edge_attach = tm.ms(5, 6);
         st->ms_emit = tm.ms(6, 7);
+        // the reference's data movement for this pass: balls in, lists out,
+        // and every candidate list (edges 8 B, triangles 12 B + 16 B
+        // orthosphere, tetrahedra 16 B + 16 B orthosphere) written and read
+        // once -- independent of how this engine avoids storing them
+        st->bytes_model = 16 * n + 8 * st->final_edges + 12 * st->final_tris +
+                          16 * st->final_tets +
+                          2 * (8 * st->cand_edges + 28 * st->cand_tris + 32 * st->cand_tets);
         if (nm == 1) {
             st->grid[0] = hg[0].gx;
             st->grid[1] = hg[0].gy;
