@@ -904,9 +904,12 @@ struct TetQueue {
     uint64_t cap;
 };
 
-template <int V>
-__global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, uint64_t lo,
-                                                       uint64_t hi) {
+// KW: link-matrix words per row this instantiation handles -- 1 for balls
+// of at most 64 upper neighbours (most balls; fewer registers, three blocks
+// per SM), kMaxW for the rest.
+template <int V, int KW>
+__global__ void __launch_bounds__(256, KW == 1 ? 3 : 2) k_tets_alpha(TetArgs A, TetQueue Q,
+                                                                     uint64_t lo, uint64_t hi) {
     __shared__ uint16_t smap[8][kMaxDeg];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
@@ -927,15 +930,16 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
         const int deg = (int)(A.eoff[p + 1] - e0);
         if (deg < 3) continue;
         const int W = (deg + 63) >> 6;
+        if ((KW == 1) != (W == 1)) continue;  // the other instantiation takes this ball
         const uint32_t *N = A.ER + e0;
         const uint64_t *Lp = A.link + A.loff[p];
         const Ball B1 = pac::ld_ball(&A.at[p]);
         const MolGrid G = A.grids[mol_of(A.mol, p)];
         for (int a = 0; a < deg - 2; a++) {
-            uint64_t ra[kMaxW];
+            uint64_t ra[KW];
             int nb = 0;
 #pragma unroll
-            for (int w = 0; w < kMaxW; w++) {
+            for (int w = 0; w < KW; w++) {
                 ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
                 nb += __popcll(ra[w]);
             }
@@ -955,10 +959,10 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
             const Ball B2 = pac::ld_ball(&A.at[v2]);
             for (int k0 = 0; k0 < nb; k0 += 32) {
                 int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
-                uint64_t m[kMaxW];
+                uint64_t m[KW];
                 int cnt = 0;
 #pragma unroll
-                for (int w = 0; w < kMaxW; w++) {
+                for (int w = 0; w < KW; w++) {
                     m[w] = (b >= 0 && w < W) ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
                                              : 0;
                     cnt += __popcll(m[w]);
@@ -980,9 +984,9 @@ __global__ void __launch_bounds__(256, 2) k_tets_alpha(TetArgs A, TetQueue Q, ui
                     const int oincl = __shfl_sync(kFull, incl, owner);
                     const int ocnt = __shfl_sync(kFull, cnt, owner);
                     const int bo = __shfl_sync(kFull, b, owner);
-                    uint64_t mo[kMaxW];
+                    uint64_t mo[KW];
 #pragma unroll
-                    for (int w = 0; w < kMaxW; w++) {
+                    for (int w = 0; w < KW; w++) {
                         uint32_t l32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
                         uint32_t h32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
                         mo[w] = ((uint64_t)h32 << 32) | l32;
@@ -1506,11 +1510,23 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
                 }
                 if (!have) continue;
                 if (e < end) {
-                    uint32_t x = e++;
-                    if (x == (uint32_t)p || x == v1 || x == v2) continue;
-                    if (dec_tri_attached<V>(A0, at, v1, v2, pac::ld_ball(&at[x]), px, py, pz, cur,
-                                            tally))
-                        have = false;
+                    if constexpr (V != pac::kExact) {
+                        // two window balls per step (independent loads)
+                        const uint32_t x0 = e, x1 = (e + 1 < end) ? e + 1 : e;
+                        e = x1 + 1;
+                        const bool ok0 = !(x0 == (uint32_t)p || x0 == v1 || x0 == v2);
+                        const bool ok1 = x1 != x0 && !(x1 == (uint32_t)p || x1 == v1 || x1 == v2);
+                        const Ball b0 = pac::ld_ball(&at[x0]), b1 = pac::ld_ball(&at[x1]);
+                        const bool t0 = pac::attached(b0, px, py, pz, cur);
+                        const bool t1 = pac::attached(b1, px, py, pz, cur);
+                        if ((ok0 && t0) || (ok1 && t1)) have = false;
+                    } else {
+                        uint32_t x = e++;
+                        if (x == (uint32_t)p || x == v1 || x == v2) continue;
+                        if (dec_tri_attached<V>(A0, at, v1, v2, pac::ld_ball(&at[x]), px, py, pz,
+                                                cur, tally))
+                            have = false;
+                    }
                     continue;
                 }
                 bool found = false;
@@ -1909,9 +1925,15 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             TetArgs TA = T;
             TA.ctr = ctrA;
             CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
-            k_tets_alpha<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 2), 256, 0, s>>>(TA, Q,
-                                                                                          lo, hi);
+            k_tets_alpha<V, 1><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 3), 256, 0, s>>>(
+                TA, Q, lo, hi);
             LAUNCH_CHECK(ctx);
+            if (maxdeg > 64) {  // balls with more than one link word per row
+                CK(cudaMemsetAsync(ctrA + C_NEXT, 0, sizeof(unsigned long long), s));
+                k_tets_alpha<V, kMaxW><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 2), 256, 0, s>>>(
+                    TA, Q, lo, hi);
+                LAUNCH_CHECK(ctx);
+            }
             unsigned long long ha[C_NCOUNTERS], used[2];
             CK(cudaMemcpyAsync(ha, ctrA, sizeof(ha), cudaMemcpyDeviceToHost, s));
             CK(cudaMemcpyAsync(used, ctr + C_SURV, sizeof(used), cudaMemcpyDeviceToHost, s));
