@@ -1045,111 +1045,175 @@ int orc_alpha_complex(const float *xyzr, uint32_t n, float sol, float alpha,
     }
     res->alpha_tris = nT;
 
-    /* ---- candidate tetrahedra + alpha filter (LD:350-591) ---- */
+    /* ---- candidate tetrahedra + alpha filter (LD:350-591) and the
+            empty-orthosphere test (LD:597-735) ---- */
     uint64_t *qcnt = XMALLOC(uint64_t, n + 1), *qoff = XMALLOC(uint64_t, n + 1);
-    uint64_t cand_q = 0;
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : cand_q)
-    for (uint32_t i = 0; i < n; i++) {
-        uint64_t b = toff[i], e = toff[i + 1], c = 0, ca = 0;
-        float o4[4];
-        uint64_t g0 = b;
-        while (g0 < e) {
-            uint32_t v2 = T2[g0];
-            uint64_t g1 = g0 + 1;
-            while (g1 < e && T2[g1] == v2) g1++;
-            for (uint64_t j = g0; j < g1; j++) {
-                uint32_t v3 = T3[j];
-                for (uint64_t k = j + 1; k < g1; k++) {
-                    uint32_t v4 = T3[k];
-                    /* (i,v3,v4) lies after k in i's sorted list, so a
-                       search over the whole list is equivalent to the
-                       reference's scan of (k, end) (LD:409-415) */
-                    if (find2(T2, T3, b, e, v3, v4) < 0) continue;
-                    if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0)
-                        continue;
-                    c++;
-                    ca += tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4);
-                }
-            }
-            g0 = g1;
-        }
-        cand_q += c;
-        qcnt[i] = ca;
-    }
-    qoff[0] = 0;
-    for (uint32_t i = 0; i < n; i++) qoff[i + 1] = qoff[i] + qcnt[i];
-    res->cand_tets = cand_q;
-    uint64_t nQ = qoff[n];
-    uint32_t *Q = XMALLOC(uint32_t, 4 * nQ);
-    float *QO = XMALLOC(float, 4 * nQ);
-#pragma omp parallel for schedule(dynamic, 64)
-    for (uint32_t i = 0; i < n; i++) {
-        uint64_t b = toff[i], e = toff[i + 1], o = qoff[i];
-        uint64_t g0 = b;
-        while (g0 < e) {
-            uint32_t v2 = T2[g0];
-            uint64_t g1 = g0 + 1;
-            while (g1 < e && T2[g1] == v2) g1++;
-            for (uint64_t j = g0; j < g1; j++) {
-                uint32_t v3 = T3[j];
-                for (uint64_t k = j + 1; k < g1; k++) {
-                    uint32_t v4 = T3[k];
-                    if (find2(T2, T3, b, e, v3, v4) < 0) continue;
-                    if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0) continue;
-                    float o4[4];
-                    if (tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4)) {
-                        Q[4 * o] = i; Q[4 * o + 1] = v2;
-                        Q[4 * o + 2] = v3; Q[4 * o + 3] = v4;
-                        memcpy(&QO[4 * o], o4, 16);
-                        o++;
+    uint32_t *Q = NULL, *FQ = NULL;
+    float *QO = NULL;
+    unsigned char *qkeep = NULL;
+    uint64_t cand_q = 0, nQ = 0, nF = 0;
+    uint64_t evals = 0, sos = 0, sosx = 0, oob = 0;
+    if (flags & ORC_TET_ORTHO) {
+        /* Each alpha tetrahedron is tested as soon as it is found and only
+           survivors are kept: at 2.5 M balls there are 6.7 G alpha
+           tetrahedra, too many to hold.  A ball is handled by one thread, in
+           enumeration order, so collecting (ball, tetrahedron) per thread and
+           placing them by per-ball survivor counts gives the reference's
+           order (ball ascending, enumeration order within a ball). */
+        int nth = 1;
+#ifdef _OPENMP
+        nth = omp_get_max_threads();
+#endif
+        uint32_t **tb = (uint32_t **)calloc((size_t)nth, sizeof(uint32_t *));
+        uint64_t *tn = (uint64_t *)calloc((size_t)nth, sizeof(uint64_t));
+        uint64_t *tcap = (uint64_t *)calloc((size_t)nth, sizeof(uint64_t));
+        uint64_t alpha_q = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : cand_q, alpha_q, evals, sos, sosx)
+        for (uint32_t i = 0; i < n; i++) {
+            int me = 0;
+#ifdef _OPENMP
+            me = omp_get_thread_num();
+#endif
+            uint64_t b = toff[i], e = toff[i + 1], c = 0, ca = 0, kept = 0;
+            float o4[4];
+            uint64_t g0 = b;
+            while (g0 < e) {
+                uint32_t v2 = T2[g0];
+                uint64_t g1 = g0 + 1;
+                while (g1 < e && T2[g1] == v2) g1++;
+                for (uint64_t j = g0; j < g1; j++) {
+                    uint32_t v3 = T3[j];
+                    for (uint64_t k = j + 1; k < g1; k++) {
+                        uint32_t v4 = T3[k];
+                        if (find2(T2, T3, b, e, v3, v4) < 0) continue;
+                        if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0) continue;
+                        c++;
+                        if (!tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4))
+                            continue;
+                        ca++;
+                        tet_ctx t;
+                        t.at = at;
+                        t.v[0] = i; t.v[1] = v2; t.v[2] = v3; t.v[3] = v4;
+                        const oatom *a1 = &at[i], *a2 = &at[v2], *a3 = &at[v3], *a4 = &at[v4];
+                        t.pa[0] = a1->x; t.pa[1] = a1->y; t.pa[2] = a1->z; t.wa = a1->r * a1->r;
+                        t.pb[0] = a2->x; t.pb[1] = a2->y; t.pb[2] = a2->z; t.wb = a2->r * a2->r;
+                        t.pc[0] = a3->x; t.pc[1] = a3->y; t.pc[2] = a3->z; t.wc = a3->r * a3->r;
+                        t.pd[0] = a4->x; t.pd[1] = a4->y; t.pd[2] = a4->z; t.wd = a4->r * a4->r;
+                        t.exact = exact;
+                        t.orientation = exact ? (float)x_orient(a1, a2, a3, a4)
+                                              : orc_orient3d(t.pa, t.pb, t.pc, t.pd);
+                        t.evals = t.sos = t.sos_exh = 0;
+                        uint64_t oob1 = 0;
+                        int viol = window_visit(&g, o4[0], o4[1], o4[2], tet_visit, &t, &oob1);
+                        evals += t.evals;
+                        sos += t.sos;
+                        sosx += t.sos_exh;
+                        if (oob1) {
+#pragma omp atomic
+                            oob += oob1;
+                        }
+                        if (viol) continue;
+                        if (tn[me] == tcap[me]) {
+                            tcap[me] = tcap[me] ? 2 * tcap[me] : 4096;
+                            tb[me] = (uint32_t *)realloc(tb[me], 16 * tcap[me]);
+                        }
+                        uint32_t *o = &tb[me][4 * tn[me]++];
+                        o[0] = i; o[1] = v2; o[2] = v3; o[3] = v4;
+                        kept++;
                     }
                 }
+                g0 = g1;
             }
-            g0 = g1;
+            cand_q += c;
+            alpha_q += ca;
+            qcnt[i] = kept;
         }
+        res->cand_tets = cand_q;
+        nQ = alpha_q;
+        qoff[0] = 0;
+        for (uint32_t i = 0; i < n; i++) qoff[i + 1] = qoff[i] + qcnt[i];
+        nF = qoff[n];
+        FQ = XMALLOC(uint32_t, 4 * nF);
+        for (uint32_t i = 0; i < n; i++) qcnt[i] = 0;
+        for (int t = 0; t < nth; t++) {
+            for (uint64_t k = 0; k < tn[t]; k++) {
+                const uint32_t *v = &tb[t][4 * k];
+                memcpy(&FQ[4 * (qoff[v[0]] + qcnt[v[0]]++)], v, 16);
+            }
+            free(tb[t]);
+        }
+        free(tb); free(tn); free(tcap);
+    } else {
+        /* as run: every alpha tetrahedron is kept, in the reference's order */
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : cand_q)
+        for (uint32_t i = 0; i < n; i++) {
+            uint64_t b = toff[i], e = toff[i + 1], c = 0, ca = 0;
+            float o4[4];
+            uint64_t g0 = b;
+            while (g0 < e) {
+                uint32_t v2 = T2[g0];
+                uint64_t g1 = g0 + 1;
+                while (g1 < e && T2[g1] == v2) g1++;
+                for (uint64_t j = g0; j < g1; j++) {
+                    uint32_t v3 = T3[j];
+                    for (uint64_t k = j + 1; k < g1; k++) {
+                        uint32_t v4 = T3[k];
+                        /* (i,v3,v4) lies after k in i's sorted list, so a
+                           search over the whole list is equivalent to the
+                           reference's scan of (k, end) (LD:409-415) */
+                        if (find2(T2, T3, b, e, v3, v4) < 0) continue;
+                        if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0)
+                            continue;
+                        c++;
+                        ca += tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4);
+                    }
+                }
+                g0 = g1;
+            }
+            cand_q += c;
+            qcnt[i] = ca;
+        }
+        qoff[0] = 0;
+        for (uint32_t i = 0; i < n; i++) qoff[i + 1] = qoff[i] + qcnt[i];
+        res->cand_tets = cand_q;
+        nQ = qoff[n];
+        Q = XMALLOC(uint32_t, 4 * nQ);
+        QO = XMALLOC(float, 4 * nQ);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (uint32_t i = 0; i < n; i++) {
+            uint64_t b = toff[i], e = toff[i + 1], o = qoff[i];
+            uint64_t g0 = b;
+            while (g0 < e) {
+                uint32_t v2 = T2[g0];
+                uint64_t g1 = g0 + 1;
+                while (g1 < e && T2[g1] == v2) g1++;
+                for (uint64_t j = g0; j < g1; j++) {
+                    uint32_t v3 = T3[j];
+                    for (uint64_t k = j + 1; k < g1; k++) {
+                        uint32_t v4 = T3[k];
+                        if (find2(T2, T3, b, e, v3, v4) < 0) continue;
+                        if (find2(T2, T3, toff[v2], toff[v2 + 1], v3, v4) < 0) continue;
+                        float o4[4];
+                        if (tet_alpha(&at[i], &at[v2], &at[v3], &at[v4], alpha, variant, o4)) {
+                            Q[4 * o] = i; Q[4 * o + 1] = v2;
+                            Q[4 * o + 2] = v3; Q[4 * o + 3] = v4;
+                            memcpy(&QO[4 * o], o4, 16);
+                            o++;
+                        }
+                    }
+                }
+                g0 = g1;
+            }
+        }
+        nF = nQ;
+        FQ = XMALLOC(uint32_t, 4 * nF);
+        memcpy(FQ, Q, 16 * nF);
+        qkeep = XMALLOC(unsigned char, 1);
     }
     res->alpha_tets = nQ;
-
-    /* ---- empty-orthosphere test of the tetrahedra (LD:597-735) ---- */
-    unsigned char *qkeep = XMALLOC(unsigned char, nQ);
-    uint64_t evals = 0, sos = 0, sosx = 0, oob = 0;
-    if (!(flags & ORC_TET_ORTHO)) memset(qkeep, 1, nQ);
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : evals, sos, sosx)
-    for (uint64_t q = 0; q < ((flags & ORC_TET_ORTHO) ? nQ : 0); q++) {
-        tet_ctx t;
-        t.at = at;
-        for (int k = 0; k < 4; k++) t.v[k] = Q[4 * q + k];
-        const oatom *a1 = &at[t.v[0]], *a2 = &at[t.v[1]], *a3 = &at[t.v[2]],
-                    *a4 = &at[t.v[3]];
-        t.pa[0] = a1->x; t.pa[1] = a1->y; t.pa[2] = a1->z; t.wa = a1->r * a1->r;
-        t.pb[0] = a2->x; t.pb[1] = a2->y; t.pb[2] = a2->z; t.wb = a2->r * a2->r;
-        t.pc[0] = a3->x; t.pc[1] = a3->y; t.pc[2] = a3->z; t.wc = a3->r * a3->r;
-        t.pd[0] = a4->x; t.pd[1] = a4->y; t.pd[2] = a4->z; t.wd = a4->r * a4->r;
-        t.exact = exact;
-        t.orientation = exact ? (float)x_orient(a1, a2, a3, a4)
-                              : orc_orient3d(t.pa, t.pb, t.pc, t.pd);
-        t.evals = t.sos = t.sos_exh = 0;
-        int viol = window_visit(&g, QO[4 * q], QO[4 * q + 1], QO[4 * q + 2],
-                                tet_visit, &t, &oob);
-        qkeep[q] = !viol;
-        evals += t.evals;
-        sos += t.sos;
-        sosx += t.sos_exh;
-    }
     res->insphere_evals = evals;
     res->sos_calls = sos;
     res->sos_exhausted = sosx;
-    uint64_t nF = 0;
-    for (uint64_t q = 0; q < nQ; q++) nF += qkeep[q];
-    uint32_t *FQ = XMALLOC(uint32_t, 4 * nF);
-    {
-        uint64_t o = 0;
-        for (uint64_t q = 0; q < nQ; q++)
-            if (qkeep[q]) {
-                memcpy(&FQ[4 * o], &Q[4 * q], 16);
-                o++;
-            }
-    }
 
     /* ---- faces of the final tetrahedra (LD:737-760, 1546-1583) ---- */
     uint32_t *TI = XMALLOC(uint32_t, 12 * nF);
