@@ -820,13 +820,71 @@ __device__ __noinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, 
     mark_face(A.faces, A.loff[v2], (deg2 + 63) >> 6, mb, mc);
 }
 
+// The 27-cell window of the orthosphere and attachment tests, visited as
+// the centre cell first (window_centre) and then ten parts (window_part):
+// the two side cells of the centre row, then the eight other x-rows -- for
+// z and y offsets (i, j) the cells (gX-1 .. gX+1, gY+j, gZ+i), clipped to
+// the grid, are consecutive in the cell order, so their balls form one range
+// of the sorted balls.  Faces before corners, so the balls nearest the
+// window centre come first and most tests end early.  Together these are the
+// reference's window (AlphaComplexLargeData.cu:621-733): the centre cell
+// through its wrapped linear index, the 26 neighbours range-checked per
+// axis; the same cells in another order, and the tests' outcome does not
+// depend on the order.
+constexpr int kWindowParts = 10;
+// rows 2..9 as (i + 1) | (j + 1) << 2, 4 bits each:
+// (0,-1) (0,1) (-1,0) (1,0) (-1,-1) (-1,1) (1,-1) (1,1)
+constexpr uint64_t kRowOrder = 0x1ull | 0x9ull << 4 | 0x4ull << 8 | 0x6ull << 12 | 0x0ull << 16 |
+                               0x8ull << 20 | 0x2ull << 24 | 0xAull << 28;
+
+// [beg, end) of window part r, or false when it lies outside the grid.
+__device__ __forceinline__ bool window_part(const MolGrid &G, const uint32_t *cellbeg, int gX,
+                                            int gY, int gZ, int r, uint32_t &beg, uint32_t &end) {
+    long long zz = gZ, yy = gY, xlo, xhi;
+    if (r < 2) {  // a side cell of the centre row
+        xlo = xhi = (long long)gX + (r == 0 ? -1 : 1);
+    } else {
+        const int code = (int)((kRowOrder >> (4 * (r - 2))) & 0xf);
+        zz += (code & 3) - 1;
+        yy += (code >> 2) - 1;
+        xlo = (long long)gX - 1;
+        xhi = (long long)gX + 1;
+    }
+    if (zz < 0 || zz >= G.gz || yy < 0 || yy >= G.gy) return false;
+    xlo = max(xlo, 0ll);
+    xhi = min(xhi, (long long)G.gx - 1);
+    if (xlo > xhi) return false;
+    const uint64_t row = G.cell_base + (uint64_t)(zz * G.gy + yy) * (uint64_t)G.gx;
+    beg = cellbeg[row + (uint64_t)xlo];
+    end = cellbeg[row + (uint64_t)xhi + 1];
+    return true;
+}
+
+// The window's centre cell as the reference reads it, through its wrapped
+// linear index cl.w: [beg, end), or an empty range (counted) when cl.w names
+// no cell (out-of-range read in the reference, AlphaComplexLargeData.cu:
+// 625-627).  When the centre (cl.x, cl.y, cl.z) lies inside the grid this is
+// the centre cell itself, which no part holds; when it lies outside, the
+// parts hold the window's in-grid cells and this is the extra cell the
+// wrapped index names.
+__device__ __forceinline__ void window_centre(const MolGrid &G, const uint32_t *cellbeg, int4 cl,
+                                              uint32_t &beg, uint32_t &end,
+                                              unsigned long long &oob) {
+    beg = end = 0;
+    if (cl.w < 0 || (uint64_t)cl.w >= G.ncell) {
+        oob++;
+        return;
+    }
+    beg = cellbeg[G.cell_base + (uint64_t)cl.w];
+    end = cellbeg[G.cell_base + (uint64_t)cl.w + 1];
+}
+
 constexpr int kLongCap = 64;   // tetrahedra handed to the cooperative scan
 constexpr int kSerialEvals = 8; // window balls a lane scans alone before handing off
 
 // Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
-// lane k < 27 owns window cell k (the centre cell through its linear index,
-// then the 26 neighbours range-checked per axis), a prefix sum over the cell
-// sizes flattens the window balls over the lanes.  Returns 1 = violated,
+// lane 0 owns the centre cell, lanes 1..10 the window's other parts, and a
+// prefix sum over their sizes flattens the window balls over the lanes.  Returns 1 = violated,
 // 2 = no violation but an exact zero, 0 = empty.
 template <int V>
 __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
@@ -837,22 +895,14 @@ __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32
                                          unsigned long long &evals, Tally &tally) {
     const int lane = threadIdx.x & 31;
     uint32_t beg = 0, cnt = 0;
-    if (lane == 0) {
-        if (cl.w >= 0 && (uint64_t)cl.w < G.ncell) {
-            uint64_t gc = G.cell_base + (uint64_t)cl.w;
-            beg = A.cellbeg[gc];
-            cnt = A.cellbeg[gc + 1] - beg;
-        }
-    } else if (lane < 27) {
-        int rr = lane - 1 + (lane >= 14 ? 1 : 0);
-        int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
-        int zz = (int)((unsigned)cl.z + (unsigned)i), yy = (int)((unsigned)cl.y + (unsigned)j),
-            xx = (int)((unsigned)cl.x + (unsigned)k);
-        if (!((zz >= G.gz) || (yy >= G.gy) || (xx >= G.gx)) && !((zz < 0) || (yy < 0) || (xx < 0))) {
-            uint64_t gc = G.cell_base + (uint64_t)lin3(xx, yy, zz, G.gx, G.gy);
-            beg = A.cellbeg[gc];
-            cnt = A.cellbeg[gc + 1] - beg;
-        }
+    if (lane == 0) {  // the centre cell
+        unsigned long long none = 0;
+        uint32_t end = 0;
+        window_centre(G, A.cellbeg, cl, beg, end, none);
+        cnt = end - beg;
+    } else if (lane <= kWindowParts) {
+        uint32_t end = 0;
+        if (window_part(G, A.cellbeg, cl.x, cl.y, cl.z, lane - 1, beg, end)) cnt = end - beg;
     }
     uint32_t incl = cnt;
     for (int o = 1; o < 32; o <<= 1) {
@@ -890,29 +940,162 @@ __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32
     return __any_sync(kFull, zero) ? 2 : 0;
 }
 
-// ---- the as-written tetrahedra in two kernels over an HBM queue ----------
-// k_tets_alpha: one warp per ball v1 (balls handed out in order from a
-// counter, over a chunk [lo, hi)).  The candidate fourth vertices of every
-// alpha triangle (v1, v2, v3) are flattened over the lanes (common bits of
-// rows a and b of v1's link matrix, checked against v2's link matrix: the
-// reference's candidate tetrahedra, AlphaComplexLargeData.cu:350-529), each
-// lane applies markRealTets to one candidate, and the passing tetrahedra are
-// appended to the queue with the cell of their orthosphere centre.
+// ---- the as-written tetrahedra: enumeration, then a scan over an HBM queue
+// Enumeration (k_tets_alpha1, k_tets_alpha_rows, through tet_row): the
+// candidate fourth vertices of every alpha triangle (v1, v2, v3) are
+// flattened over the lanes (common bits of rows a and b of v1's link matrix,
+// checked against v2's link matrix: the reference's candidate tetrahedra,
+// AlphaComplexLargeData.cu:350-529), each lane applies markRealTets to one
+// candidate, and the passing tetrahedra are appended to the queue with the
+// cell of their orthosphere centre.
 struct TetQueue {
     uint2 *pk;        // (ball v1, a | b << 8 | c << 16)
     int4 *cell;       // (gridX, gridY, gridZ, linear centre index)
     uint64_t cap;
 };
 
-// KW: link-matrix words per row this instantiation handles -- 1 for balls
-// of at most 64 upper neighbours (most balls; fewer registers, three blocks
-// per SM), kMaxW for the rest.
-template <int V, int KW>
-__global__ void __launch_bounds__(256, KW == 1 ? 3 : 2) k_tets_alpha(TetArgs A, TetQueue Q,
-                                                                     uint64_t lo, uint64_t hi) {
-    __shared__ uint16_t smap[8][kMaxDeg];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+// One row a of ball v1's candidate tetrahedra (v1, v2 = N[a], v3, v4).  The
+// caller has staged the balls of v1's upper neighbours in sb (indexed like
+// N, at least for c > a); L holds v1's link rows (W words each, shared or
+// global memory).  v2's neighbour list and link rows are staged here, in
+// sN2 and sL2 (when they fit: at most L2CAP words), so the candidate loop
+// reads no global memory but the queue it appends to.
+template <int V, int KW, int L2CAP>
+__device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uint64_t p, int a,
+                                        int deg, int W, const uint32_t *N, const uint64_t *L,
+                                        const float4 *sb, uint32_t *sN2, uint64_t *sL2,
+                                        uint16_t *smap, const Ball B1, const MolGrid &G,
+                                        unsigned long long &cand_acc,
+                                        unsigned long long &alpha_acc, Tally &tally) {
+    const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
+    uint64_t ra[KW];
+    int nb = 0;
+#pragma unroll
+    for (int w = 0; w < KW; w++) {
+        ra[w] = w < W ? L[(uint64_t)a * W + w] : 0;
+        nb += __popcll(ra[w]);
+    }
+    if (nb < 2) return;
+    const uint32_t v2 = __ldg(&N[a]);
+    const uint64_t e2 = A.eoff[v2];
+    const int deg2 = (int)(A.eoff[v2 + 1] - e2);
+    const int W2 = (deg2 + 63) >> 6;
+    const uint64_t *L2 = A.link + A.loff[v2];
+    const bool l2s = deg2 * W2 <= L2CAP;  // v2's rows staged
+    for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
+    if (l2s)
+        for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2[k];
+    __syncwarp();
+    for (int c = a + 1 + lane; c < deg; c += 32) {
+        const uint32_t x = __ldg(&N[c]);
+        int lo2 = 0, n2 = deg2;  // lower bound of x in v2's list
+        while (n2 > 0) {
+            const int h = n2 >> 1;
+            if (sN2[lo2 + h] < x) {
+                lo2 += h + 1;
+                n2 -= h + 1;
+            } else {
+                n2 = h;
+            }
+        }
+        smap[c] = (lo2 < deg2 && sN2[lo2] == x) ? (uint16_t)lo2 : (uint16_t)0xffff;
+    }
+    __syncwarp();
+    const float4 b2 = sb[a];
+    const Ball B2{b2.x, b2.y, b2.z, b2.w};
+    for (int k0 = 0; k0 < nb; k0 += 32) {
+        const int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
+        uint64_t m[KW];
+        int cnt = 0;
+#pragma unroll
+        for (int w = 0; w < KW; w++) {
+            m[w] = (b >= 0 && w < W) ? (ra[w] & L[(uint64_t)b * W + w] & above_mask(b, w)) : 0;
+            cnt += __popcll(m[w]);
+        }
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        for (int base = 0; base < total; base += 32) {
+            const int s = base + lane;
+            int lo3 = 0;
+            for (int step = 16; step; step >>= 1) {
+                int v = __shfl_sync(kFull, incl, lo3 + step - 1);
+                if (v <= s) lo3 += step;
+            }
+            const int owner = lo3 & 31;
+            const int oincl = __shfl_sync(kFull, incl, owner);
+            const int ocnt = __shfl_sync(kFull, cnt, owner);
+            const int bo = __shfl_sync(kFull, b, owner);
+            uint64_t mo[KW];
+#pragma unroll
+            for (int w = 0; w < KW; w++) {
+                uint32_t l32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
+                uint32_t h32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
+                mo[w] = ((uint64_t)h32 << 32) | l32;
+            }
+            bool pass4 = false, passA = false;
+            int c = -1;
+            int4 cell = make_int4(0, 0, 0, 0);
+            if (s < total) {
+                c = select_bit(mo, W, s - (oincl - ocnt));
+                const int mb = smap[bo], mc = smap[c];
+                if (mb != 0xffff && mc != 0xffff) {
+                    const uint64_t at2 = (uint64_t)mb * W2 + (mc >> 6);
+                    const uint64_t word = l2s ? sL2[at2] : __ldg(&L2[at2]);
+                    pass4 = (word >> (mc & 63)) & 1ull;
+                }
+                if (pass4) {
+                    const float4 b3 = sb[bo], b4 = sb[c];
+                    const Ball B3{b3.x, b3.y, b3.z, b3.w}, B4{b4.x, b4.y, b4.z, b4.w};
+                    float4 sphere;
+                    passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
+                    if (passA) {
+                        int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
+                        int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
+                        int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
+                        cell = make_int4(gridX, gridY, gridZ, lin3(gridX, gridY, gridZ, G.gx, G.gy));
+                    }
+                }
+            }
+            const unsigned m4 = __ballot_sync(kFull, pass4);
+            const unsigned mA = __ballot_sync(kFull, passA);
+            unsigned long long qbase = 0;
+            if (lane == 0 && mA) qbase = atomicAdd(&A.ctr[C_SURV], (unsigned long long)__popc(mA));
+            qbase = __shfl_sync(kFull, qbase, 0);
+            if (passA) {
+                uint64_t pos = qbase + __popc(mA & lt_mask);
+                if (pos < Q.cap) {
+                    Q.pk[pos] = make_uint2((uint32_t)p,
+                                           (uint32_t)a | ((uint32_t)bo << 8) | ((uint32_t)c << 16));
+                    Q.cell[pos] = cell;
+                }
+            }
+            if (lane == 0) {
+                cand_acc += __popc(m4);
+                alpha_acc += __popc(mA);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// k_tets_alpha1: balls of at most 64 upper neighbours (one link word per
+// row; most balls), one warp per ball, balls handed out from a counter over
+// the chunk [lo, hi).  The balls of v1's neighbours and v1's link rows are
+// staged in shared memory once per ball.
+template <int V>
+__global__ void __launch_bounds__(256, 3) k_tets_alpha1(TetArgs A, TetQueue Q, uint64_t lo,
+                                                        uint64_t hi) {
+    __shared__ float4 sb[8][64];          // balls of v1's upper neighbours
+    __shared__ uint64_t sL[8][64];        // v1's link rows
+    __shared__ uint64_t sL2[8][64];       // v2's link rows (when they fit)
+    __shared__ uint32_t sN2[8][kMaxDeg];  // v2's upper neighbours
+    __shared__ uint16_t smap[8][64];      // position of N[c] in v2's list, 0xffff: absent
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
     Tally tally;
     while (true) {
@@ -928,112 +1111,83 @@ __global__ void __launch_bounds__(256, KW == 1 ? 3 : 2) k_tets_alpha(TetArgs A, 
         if (p >= hi) break;
         const uint64_t e0 = A.eoff[p];
         const int deg = (int)(A.eoff[p + 1] - e0);
-        if (deg < 3) continue;
-        const int W = (deg + 63) >> 6;
-        if ((KW == 1) != (W == 1)) continue;  // the other instantiation takes this ball
+        if (deg < 3 || deg > 64) continue;  // k_tets_alpha_rows takes the larger balls
         const uint32_t *N = A.ER + e0;
         const uint64_t *Lp = A.link + A.loff[p];
+        for (int c = lane; c < deg; c += 32) {
+            sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
+            sL[wib][c] = Lp[c];
+        }
         const Ball B1 = pac::ld_ball(&A.at[p]);
         const MolGrid G = A.grids[mol_of(A.mol, p)];
-        for (int a = 0; a < deg - 2; a++) {
-            uint64_t ra[KW];
-            int nb = 0;
-#pragma unroll
-            for (int w = 0; w < KW; w++) {
-                ra[w] = w < W ? Lp[(uint64_t)a * W + w] : 0;
-                nb += __popcll(ra[w]);
-            }
-            if (nb < 2) continue;
-            const uint32_t v2 = __ldg(&N[a]);
-            const uint64_t e2 = A.eoff[v2];
-            const int deg2 = (int)(A.eoff[v2 + 1] - e2);
-            const int W2 = (deg2 + 63) >> 6;
-            const uint64_t *L2 = A.link + A.loff[v2];
-            for (int c = a + 1 + lane; c < deg; c += 32) {
-                uint32_t x = __ldg(&N[c]);
-                int pos = lbound(A.ER + e2, deg2, x);
-                smap[wib][c] = (pos < deg2 && __ldg(&A.ER[e2 + pos]) == x) ? (uint16_t)pos
-                                                                           : (uint16_t)0xffff;
-            }
-            __syncwarp();
-            const Ball B2 = pac::ld_ball(&A.at[v2]);
-            for (int k0 = 0; k0 < nb; k0 += 32) {
-                int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
-                uint64_t m[KW];
-                int cnt = 0;
-#pragma unroll
-                for (int w = 0; w < KW; w++) {
-                    m[w] = (b >= 0 && w < W) ? (ra[w] & Lp[(uint64_t)b * W + w] & above_mask(b, w))
-                                             : 0;
-                    cnt += __popcll(m[w]);
-                }
-                int incl = cnt;
-                for (int o = 1; o < 32; o <<= 1) {
-                    int v = __shfl_up_sync(kFull, incl, o);
-                    if (lane >= o) incl += v;
-                }
-                const int total = __shfl_sync(kFull, incl, 31);
-                for (int base = 0; base < total; base += 32) {
-                    const int s = base + lane;
-                    int lo2 = 0;
-                    for (int step = 16; step; step >>= 1) {
-                        int v = __shfl_sync(kFull, incl, lo2 + step - 1);
-                        if (v <= s) lo2 += step;
-                    }
-                    const int owner = lo2 & 31;
-                    const int oincl = __shfl_sync(kFull, incl, owner);
-                    const int ocnt = __shfl_sync(kFull, cnt, owner);
-                    const int bo = __shfl_sync(kFull, b, owner);
-                    uint64_t mo[KW];
-#pragma unroll
-                    for (int w = 0; w < KW; w++) {
-                        uint32_t l32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
-                        uint32_t h32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
-                        mo[w] = ((uint64_t)h32 << 32) | l32;
-                    }
-                    bool pass4 = false, passA = false;
-                    int c = -1;
-                    int4 cell = make_int4(0, 0, 0, 0);
-                    if (s < total) {
-                        c = select_bit(mo, W, s - (oincl - ocnt));
-                        const int mb = smap[wib][bo], mc = smap[wib][c];
-                        pass4 = mb != 0xffff && mc != 0xffff &&
-                                ((__ldg(&L2[(uint64_t)mb * W2 + (mc >> 6)]) >> (mc & 63)) & 1ull);
-                        if (pass4) {
-                            const Ball B3 = pac::ld_ball(&A.at[__ldg(&N[bo])]);
-                            const Ball B4 = pac::ld_ball(&A.at[__ldg(&N[c])]);
-                            float4 sphere;
-                            passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
-                            if (passA) {
-                                int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
-                                int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
-                                int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
-                                cell = make_int4(gridX, gridY, gridZ,
-                                                 lin3(gridX, gridY, gridZ, G.gx, G.gy));
-                            }
-                        }
-                    }
-                    const unsigned m4 = __ballot_sync(kFull, pass4);
-                    const unsigned mA = __ballot_sync(kFull, passA);
-                    unsigned long long qbase = 0;
-                    if (lane == 0 && mA) qbase = atomicAdd(&A.ctr[C_SURV], (unsigned long long)__popc(mA));
-                    qbase = __shfl_sync(kFull, qbase, 0);
-                    if (passA) {
-                        uint64_t pos = qbase + __popc(mA & lt_mask);
-                        if (pos < Q.cap) {
-                            Q.pk[pos] = make_uint2((uint32_t)p, (uint32_t)a | ((uint32_t)bo << 8) |
-                                                                    ((uint32_t)c << 16));
-                            Q.cell[pos] = cell;
-                        }
-                    }
-                    if (lane == 0) {
-                        cand_acc += __popc(m4);
-                        alpha_acc += __popc(mA);
-                    }
-                }
-            }
-            __syncwarp();
+        __syncwarp();
+        for (int a = 0; a < deg - 2; a++)
+            tet_row<V, 1, 64>(A, Q, p, a, deg, 1, N, sL[wib], sb[wib], sN2[wib], sL2[wib],
+                              smap[wib], B1, G, cand_acc, alpha_acc, tally);
+        __syncwarp();
+    }
+    flush_tally<V>(tally, A.gctr);
+    if (lane == 0) {
+        bump(A.ctr, C_CAND_Q, cand_acc);
+        bump(A.ctr, C_ALPHA_Q, alpha_acc);
+    }
+}
+
+// Rows of the candidate enumeration per ball with more than 64 upper
+// neighbours (deg - 2), 0 for the others: the work units of
+// k_tets_alpha_rows.
+__global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, uint32_t *rows) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint64_t deg = eoff[p + 1] - eoff[p];
+    rows[p] = deg > 64 ? (uint32_t)(deg - 2) : 0u;
+}
+
+// k_tets_alpha_rows: balls of more than 64 upper neighbours, one warp per
+// (ball, row a) -- such balls hold many candidates each, and a whole ball
+// per warp left most warps idle behind a few.  uoff[p] is the exclusive
+// prefix of k_heavy_rows; units of the chunk [lo, hi) are handed out from a
+// counter.  Per unit the balls of v1's neighbours beyond a are staged.
+template <int V>
+__global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
+                                                            uint64_t hi, const uint64_t *uoff) {
+    __shared__ float4 sb[4][kMaxDeg];
+    __shared__ uint64_t sL2[4][512];  // v2's link rows when they fit (else read in place)
+    __shared__ uint32_t sN2[4][kMaxDeg];
+    __shared__ uint16_t smap[4][kMaxDeg];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned long long cand_acc = 0, alpha_acc = 0;
+    Tally tally;
+    const uint64_t u0 = uoff[lo], u1 = uoff[hi];
+    while (true) {
+        uint64_t u = 0;
+        if (lane == 0) {
+            u = (*(volatile unsigned long long *)&A.ctr[C_SURV] > Q.cap)
+                    ? u1
+                    : u0 + atomicAdd(&A.ctr[C_NEXT], 1ull);
         }
+        u = __shfl_sync(kFull, u, 0);
+        if (u >= u1) break;
+        // the ball: largest p in [lo, hi) with uoff[p] <= u
+        uint64_t pl = lo, ph = hi;  // uoff[pl] <= u < uoff[ph]
+        while (ph - pl > 1) {
+            const uint64_t mid = (pl + ph) >> 1;
+            if (uoff[mid] <= u) pl = mid;
+            else ph = mid;
+        }
+        const uint64_t p = pl;
+        const int a = (int)(u - uoff[p]);
+        const uint64_t e0 = A.eoff[p];
+        const int deg = (int)(A.eoff[p + 1] - e0);
+        const int W = (deg + 63) >> 6;
+        const uint32_t *N = A.ER + e0;
+        const uint64_t *Lp = A.link + A.loff[p];
+        for (int c = a + lane; c < deg; c += 32) sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
+        const Ball B1 = pac::ld_ball(&A.at[p]);
+        const MolGrid G = A.grids[mol_of(A.mol, p)];
+        __syncwarp();
+        tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, N, Lp, sb[wib], sN2[wib], sL2[wib],
+                                          smap[wib], B1, G, cand_acc, alpha_acc, tally);
     }
     flush_tally<V>(tally, A.gctr);
     if (lane == 0) {
@@ -1137,14 +1291,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
                 q = 0;
                 nev = 0;
                 zero = false;
-                if (cl.w >= 0 && (uint64_t)cl.w < G->ncell) {
-                    uint64_t gc = G->cell_base + (uint64_t)cl.w;
-                    e = A.cellbeg[gc];
-                    end = A.cellbeg[gc + 1];
-                } else {
-                    e = end = 0;
-                    oob++;
-                }
+                window_centre(*G, A.cellbeg, cl, e, end, oob);
                 have = true;
             }
             head = min(tail, head + (uint64_t)__popc(want));
@@ -1217,20 +1364,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             }
         }
         bool found = false;
-        const int Ggx = G->gx, Ggy = G->gy, Ggz = G->gz;
-        while (q < 26 && !found) {
-            q++;
-            int rr = q - 1 + (q >= 14 ? 1 : 0);
-            int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
-            int zz = (int)((unsigned)gZ + (unsigned)i), yy = (int)((unsigned)gY + (unsigned)j),
-                xx = (int)((unsigned)gX + (unsigned)k);
-            if ((zz >= Ggz) || (yy >= Ggy) || (xx >= Ggx)) continue;
-            if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
-            uint64_t gc = G->cell_base + (uint64_t)lin3(xx, yy, zz, Ggx, Ggy);
-            e = A.cellbeg[gc];
-            end = A.cellbeg[gc + 1];
-            found = true;
-        }
+        while (q < kWindowParts && !found) found = window_part(*G, A.cellbeg, gX, gY, gZ, q++, e, end);
         if (!found) {
             const uint32_t *N = A.ER + A.eoff[p];
             const int deg = (int)(A.eoff[p + 1] - A.eoff[p]);
@@ -1491,15 +1625,9 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
                         gX = pac::cell_coord(p1.x, G->minx, G->step);
                         gY = pac::cell_coord(p1.y, G->miny, G->step);
                         gZ = pac::cell_coord(p1.z, G->minz, G->step);
-                        int cc = lin3(gX, gY, gZ, G->gx, G->gy);
                         q = 0;
-                        if (cc >= 0 && (uint64_t)cc < G->ncell) {
-                            e = cellbeg[G->cell_base + cc];
-                            end = cellbeg[G->cell_base + cc + 1];
-                        } else {
-                            e = end = 0;
-                            oob++;
-                        }
+                        window_centre(*G, cellbeg, make_int4(gX, gY, gZ, lin3(gX, gY, gZ, G->gx, G->gy)),
+                                      e, end, oob);
                         have = true;
                     }
                     head = min(qn, head + __popc(want));
@@ -1530,20 +1658,8 @@ __global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 
                     continue;
                 }
                 bool found = false;
-                const int Ggx = G->gx, Ggy = G->gy, Ggz = G->gz;
-                while (q < 26 && !found) {
-                    q++;
-                    int rr = q - 1 + (q >= 14 ? 1 : 0);
-                    int i = rr / 9 - 1, j = (rr / 3) % 3 - 1, k = rr % 3 - 1;
-                    int zz = (int)((unsigned)gZ + (unsigned)i), yy = (int)((unsigned)gY + (unsigned)j),
-                        xx = (int)((unsigned)gX + (unsigned)k);
-                    if ((zz >= Ggz) || (yy >= Ggy) || (xx >= Ggx)) continue;
-                    if ((zz < 0) || (yy < 0) || (xx < 0)) continue;
-                    uint64_t gc = G->cell_base + (uint64_t)lin3(xx, yy, zz, Ggx, Ggy);
-                    e = cellbeg[gc];
-                    end = cellbeg[gc + 1];
-                    found = true;
-                }
+                while (q < kWindowParts && !found)
+                    found = window_part(*G, cellbeg, gX, gY, gZ, q++, e, end);
                 if (!found) {
                     atomicOr((unsigned long long *)&faces[lp + (uint64_t)ta * W + (tb >> 6)],
                              1ull << (tb & 63));
@@ -1918,6 +2034,19 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
         CK(cudaMemsetAsync(T.tcount, 0, sizeof(uint32_t) * n, s));
+        // work units of the balls with more than 64 upper neighbours
+        uint32_t *hrows = ar.alloc_n<uint32_t>(n);
+        uint64_t *uoff = ar.alloc_n<uint64_t>(n + 1);
+        if (!hrows || !uoff) return PAC_ERR_OOM;
+        uint64_t heavy_units = 0;
+        if (maxdeg > 64) {
+            k_heavy_rows<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, hrows);
+            LAUNCH_CHECK(ctx);
+            rc = exclusive_scan(ctx, hrows, n, uoff);
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(&heavy_units, uoff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
         unsigned long long cand_total = 0, alpha_total = 0;
         uint64_t lo = 0, chunk = n;
         while (lo < n) {
@@ -1925,13 +2054,12 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             TetArgs TA = T;
             TA.ctr = ctrA;
             CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
-            k_tets_alpha<V, 1><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 3), 256, 0, s>>>(
+            k_tets_alpha1<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 3), 256, 0, s>>>(
                 TA, Q, lo, hi);
             LAUNCH_CHECK(ctx);
-            if (maxdeg > 64) {  // balls with more than one link word per row
+            if (heavy_units) {  // balls with more than 64 upper neighbours, by rows
                 CK(cudaMemsetAsync(ctrA + C_NEXT, 0, sizeof(unsigned long long), s));
-                k_tets_alpha<V, kMaxW><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 2), 256, 0, s>>>(
-                    TA, Q, lo, hi);
+                k_tets_alpha_rows<V><<<148 * 4, 128, 0, s>>>(TA, Q, lo, hi, uoff);
                 LAUNCH_CHECK(ctx);
             }
             unsigned long long ha[C_NCOUNTERS], used[2];

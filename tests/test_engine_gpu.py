@@ -289,3 +289,27 @@ def test_chunked_tetrahedron_queue(pac, orc):
         r = eng.alpha_complex(balls, 1.4, 1.0)
     _same(r, e, t, q)
     assert r.stats["alpha_tets"] == st["alpha_tets"] and r.stats["cand_tets"] == st["cand_tets"]
+
+
+@pytest.mark.slow
+def test_assembly_2p5m_matches_restatement_digest(pac):
+    """The north star's large single pass: 2.5M balls (400 globules of 6,250
+    in an 8 x 10 x 5 grid at 60 A pitch), sol 1.4, alpha 1, as written, in
+    one call (the tetrahedron queue runs in chunks); lists and stage counts
+    against the restatement's digests (tests/golden/make_assembly_digest.py)."""
+    import hashlib
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "assembly_2p5m.json")))
+    balls = pac.assembly()
+    assert hashlib.sha256(balls.tobytes()).hexdigest() == man["input_sha256"]
+
+    def sha(a):
+        return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint32).tobytes()).hexdigest()
+    rec = man["as-written"]
+    with _engine(pac, 0, "as-written") as eng:
+        r = eng.alpha_complex(balls, 1.4, 1.0)
+    assert [len(r.edges), len(r.tris), len(r.tets)] == rec["counts"]
+    assert [sha(r.edges), sha(r.tris), sha(r.tets)] == rec["sha256"]
+    for k in ("cand_edges", "alpha_edges", "cand_tris", "alpha_tris", "cand_tets", "alpha_tets"):
+        assert r.stats[k] == rec["stats"][k], k
+    print("2.5M assembly: %.1f ms, %d simplices" % (r.stats["ms_total"], sum(rec["counts"])))
