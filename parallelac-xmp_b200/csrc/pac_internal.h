@@ -72,6 +72,10 @@ struct Ctx {
     // grows, never shrinks, reused by every call
     void *pinned = nullptr;
     size_t pinned_size = 0;
+    // bytes for the alpha-tetrahedron queue, fixed at the context's first
+    // pass (a quarter of the memory free then, at most 8 GiB), so that later
+    // passes lay out the pool the same way
+    uint64_t queue_bytes = 0;
 };
 
 int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uint32_t *d_edges,

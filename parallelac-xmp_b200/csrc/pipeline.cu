@@ -1133,21 +1133,23 @@ __global__ void __launch_bounds__(256, 3) k_tets_alpha1(TetArgs A, TetQueue Q, u
     }
 }
 
-// Rows of the candidate enumeration per ball with more than 64 upper
-// neighbours (deg - 2), 0 for the others: the work units of
-// k_tets_alpha_rows.
+// Work units of k_tets_alpha_rows per ball: ceil((deg - 2) / kUnitRows)
+// groups of rows for a ball with more than 64 upper neighbours, 0 for the
+// others.
+constexpr int kUnitRows = 8;
 __global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, uint32_t *rows) {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const uint64_t deg = eoff[p + 1] - eoff[p];
-    rows[p] = deg > 64 ? (uint32_t)(deg - 2) : 0u;
+    rows[p] = deg > 64 ? (uint32_t)((deg - 2 + kUnitRows - 1) / kUnitRows) : 0u;
 }
 
 // k_tets_alpha_rows: balls of more than 64 upper neighbours, one warp per
-// (ball, row a) -- such balls hold many candidates each, and a whole ball
-// per warp left most warps idle behind a few.  uoff[p] is the exclusive
-// prefix of k_heavy_rows; units of the chunk [lo, hi) are handed out from a
-// counter.  Per unit the balls of v1's neighbours beyond a are staged.
+// (ball, group of kUnitRows rows) -- such balls hold many candidates each,
+// and a whole ball per warp left most warps idle behind a few.  uoff[p] is
+// the exclusive prefix of k_heavy_rows; units of the chunk [lo, hi) are
+// handed out from a counter.  Per unit the balls of v1's neighbours beyond
+// its first row are staged.
 template <int V>
 __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
                                                             uint64_t hi, const uint64_t *uoff) {
@@ -1176,18 +1178,21 @@ __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue 
             else ph = mid;
         }
         const uint64_t p = pl;
-        const int a = (int)(u - uoff[p]);
+        const int a0 = (int)(u - uoff[p]) * kUnitRows;
         const uint64_t e0 = A.eoff[p];
         const int deg = (int)(A.eoff[p + 1] - e0);
         const int W = (deg + 63) >> 6;
         const uint32_t *N = A.ER + e0;
         const uint64_t *Lp = A.link + A.loff[p];
-        for (int c = a + lane; c < deg; c += 32) sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
+        for (int c = a0 + lane; c < deg; c += 32) sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
         const Ball B1 = pac::ld_ball(&A.at[p]);
         const MolGrid G = A.grids[mol_of(A.mol, p)];
         __syncwarp();
-        tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, N, Lp, sb[wib], sN2[wib], sL2[wib],
-                                          smap[wib], B1, G, cand_acc, alpha_acc, tally);
+        const int a1 = min(a0 + kUnitRows, deg - 2);
+        for (int a = a0; a < a1; a++)
+            tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, N, Lp, sb[wib], sN2[wib], sL2[wib],
+                                   smap[wib], B1, G, cand_acc, alpha_acc, tally);
+        __syncwarp();
     }
     flush_tally<V>(tally, A.gctr);
     if (lane == 0) {
