@@ -398,7 +398,7 @@ def main():
             "what": "one alpha_complex_device call, CUDA events; as written, strict"}
         del d_ab
 
-    # ---- roofline of the dominant stage (k_tets_alpha + k_tets_scan)
+    # ---- roofline of the dominant stage (enumeration + orthosphere scan)
     s0 = stats[-1]
     tet_ms = sum(s["ms_tets"] for s in stats) / len(stats)
     # reference byte model: every candidate tetrahedron (16 B) and its
@@ -469,7 +469,7 @@ def main():
                 "host_wall_ms_per_step": 1e3 * sum(e2e_wall) / len(e2e_wall)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "tetrahedron stage (k_tets_alpha + k_tets_scan + k_sos_resolve)",
+                     "kernel": "tetrahedron stage (k_tets_alpha1 + k_tets_alpha_rows + k_tets_scan + k_sos_resolve)",
                      "bytes_model": "64 B x candidate tetrahedra (the reference's tetrahedron "
                                     "and orthosphere lists written and read once)",
                      "kernel_ms": tet_ms},
