@@ -106,8 +106,17 @@ typedef struct {
     int tet_mode;    /* pac_tet_mode, default PAC_TETS_AS_WRITTEN */
     int predicates;  /* pac_pred_mode, default PAC_PRED_REFCOMPAT */
     int order;       /* pac_order, default PAC_ORDER_REFERENCE */
-    int autotune;    /* 1: pick launch shapes by measurement (batched mode) */
+    /* 1: pick launch shapes by measurement.  The context's first passes
+       each try one candidate shape (the orthosphere scan's hand-off
+       threshold and blocks per SM; 8 candidates), timing the tetrahedron
+       stage; later passes use the fastest.  Every shape gives the same
+       lists, so tuning passes return correct results too. */
+    int autotune;
     int verbose;     /* 1: print per-stage timings to stderr */
+    /* reserved_i[0]: if > 0, the scan's hand-off threshold (window balls a
+       lane tests alone before the whole warp takes the tetrahedron; default:
+       never); reserved_i[1]: if > 0, the scan's blocks per SM (default 4).
+       Either one turns the autotuner off. */
     int reserved_i[9];
     /* reserved_u[0]: if nonzero, the number of alpha tetrahedra the pass
        queues per chunk (default: a quarter of free device memory, at most

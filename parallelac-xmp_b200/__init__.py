@@ -155,7 +155,8 @@ class Engine:
     """A pac_ctx: one CUDA stream and device memory pool on one device."""
 
     def __init__(self, device=0, formula="upstream", tet_mode="as-written", predicates="strict",
-                 order="reference", verbose=False, queue_entries=None):
+                 order="reference", verbose=False, queue_entries=None, autotune=False,
+                 handoff=None, scan_blocks=None):
         L = _lib()
         o = Options()
         L.pac_default_options(ctypes.byref(o))
@@ -167,6 +168,11 @@ class Engine:
         o.verbose = int(verbose)
         if queue_entries:
             o.reserved_u[0] = int(queue_entries)  # alpha-tetrahedron queue size (testing)
+        o.autotune = int(bool(autotune))
+        if handoff:
+            o.reserved_i[0] = int(handoff)  # launch-shape overrides
+        if scan_blocks:
+            o.reserved_i[1] = int(scan_blocks)
         self._ctx = ctypes.c_void_p()
         _check(L.pac_create(ctypes.byref(self._ctx), ctypes.byref(o)))
 

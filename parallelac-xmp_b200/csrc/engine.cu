@@ -95,6 +95,16 @@ __global__ void k_check_finite(const float4 *b, uint64_t n, int *bad) {
     if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
 }
 
+// Launch shapes for the autotuner (pac_options.autotune): the cooperative
+// hand-off threshold of the orthosphere scan (kNoHandoff: a lane finishes
+// every tetrahedron it takes) and its blocks per SM.  The first is the
+// default: on the 100k-ball globule the hand-off cost more than it saved
+// (30.1 ms without it, 31.2 at 32 balls, 34.3 at 8).
+constexpr int kNoHandoff = 1 << 30;
+constexpr pac::LaunchShape kShapes[] = {{kNoHandoff, 4}, {kNoHandoff, 3}, {kNoHandoff, 6},
+                                        {kNoHandoff, 2}, {256, 4}, {128, 4}, {64, 4}, {32, 4}};
+constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+
 int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
         const uint64_t *h_off, float sol, float alpha, pac::PassOutput &out, pac_stats *st) {
     pac::Ctx &c = ctx->c;
@@ -121,11 +131,35 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
     uint64_t qbytes = c.queue_bytes;
     if (c.opt.reserved_u[0]) qbytes = c.opt.reserved_u[0] * 24ull;  // test hook: entries
     pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 24,
-                            c.opt.predicates == PAC_PRED_EXACT};
+                            c.opt.predicates == PAC_PRED_EXACT, kShapes[0].handoff,
+                            kShapes[0].scan_blocks};
+    // launch shapes: the caller's overrides, else the autotuner's current
+    // candidate or its choice, else the defaults
+    int cand = -1;
+    if (c.opt.autotune && !c.opt.reserved_i[0] && !c.opt.reserved_i[1]) {
+        cand = c.tuner.best >= 0 ? c.tuner.best : c.tuner.next;
+        cfg.handoff = kShapes[cand].handoff;
+        cfg.scan_blocks = kShapes[cand].scan_blocks;
+    }
+    if (c.opt.reserved_i[0] > 0) cfg.handoff = c.opt.reserved_i[0];
+    if (c.opt.reserved_i[1] > 0) cfg.scan_blocks = c.opt.reserved_i[1];
+    pac_stats local;
+    pac_stats *sp = st ? st : &local;
     pac::PassInput in{d_balls, n, n_mol, h_off, sol, alpha};
     int rc = (c.opt.predicates == PAC_PRED_REFCOMPAT_FMA)
-                 ? pac_fma::run_pass(c, cfg, in, out, st)
-                 : pac_strict::run_pass(c, cfg, in, out, st);
+                 ? pac_fma::run_pass(c, cfg, in, out, sp)
+                 : pac_strict::run_pass(c, cfg, in, out, sp);
+    if (rc == PAC_OK && cand >= 0 && c.tuner.best < 0) {
+        // every candidate gives the same lists; keep the fastest tetrahedron
+        // stage once each has run on this context's work
+        c.tuner.ms[cand] = sp->ms_tets;
+        if (++c.tuner.next == kNumShapes) {
+            int b = 0;
+            for (int k = 1; k < kNumShapes; k++)
+                if (c.tuner.ms[k] < c.tuner.ms[b]) b = k;
+            c.tuner.best = b;
+        }
+    }
     if (rc == PAC_OK) {
         e = cudaStreamSynchronize(c.stream);
         if (e != cudaSuccess)

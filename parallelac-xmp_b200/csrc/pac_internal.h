@@ -42,6 +42,19 @@ struct PipelineConfig {
     int verbose;
     uint64_t queue_entries;  // alpha tetrahedra queued per chunk (24 B each)
     bool exact;              // decision-exact predicates (strict flavour only)
+    // launch shapes (the output does not depend on them)
+    int handoff;      // window balls a scan lane tests alone before the warp takes over
+    int scan_blocks;  // k_tets_scan blocks per SM
+};
+
+// Launch shapes the autotuner tries, and its state per context.
+struct LaunchShape {
+    int handoff, scan_blocks;
+};
+struct Tuner {
+    int next = 0;          // next candidate to measure
+    int best = -1;         // chosen candidate once all are measured
+    double ms[16] = {0};   // tetrahedron-stage time of each candidate
 };
 
 // Inputs of one device pass over one or more molecules.
@@ -76,6 +89,7 @@ struct Ctx {
     // pass (a quarter of the memory free then, at most 8 GiB), so that later
     // passes lay out the pool the same way
     uint64_t queue_bytes = 0;
+    Tuner tuner;
 };
 
 int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uint32_t *d_edges,

@@ -659,6 +659,7 @@ struct TetArgs {
     uint32_t *tets_out;   // as-run fill: sorted-space vertex quadruples
     unsigned long long *ctr;
     unsigned long long *gctr;  // the pass's counters (ctr may be a chunk's)
+    int handoff;               // scan: window balls a lane tests alone
 };
 
 __device__ __forceinline__ void mark_face(uint64_t *F, uint64_t row_base, int W, int a, int b) {
@@ -880,7 +881,6 @@ __device__ __forceinline__ void window_centre(const MolGrid &G, const uint32_t *
 }
 
 constexpr int kLongCap = 64;   // tetrahedra handed to the cooperative scan
-constexpr int kSerialEvals = 8; // window balls a lane scans alone before handing off
 
 // Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
 // lane 0 owns the centre cell, lanes 1..10 the window's other parts, and a
@@ -955,9 +955,9 @@ struct TetQueue {
 };
 
 // One row a of ball v1's candidate tetrahedra (v1, v2 = N[a], v3, v4).  The
-// caller has staged the balls of v1's upper neighbours in sb (indexed like
-// N, at least for c > a); L holds v1's link rows (W words each, shared or
-// global memory).  v2's neighbour list and link rows are staged here, in
+// caller has staged v1's upper neighbours in N and their balls in sb (both
+// in shared memory, indexed by position, at least from a on); L holds v1's
+// link rows (W words each, shared or global memory).  v2's neighbour list and link rows are staged here, in
 // sN2 and sL2 (when they fit: at most L2CAP words), so the candidate loop
 // reads no global memory but the queue it appends to.
 template <int V, int KW, int L2CAP>
@@ -977,7 +977,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
         nb += __popcll(ra[w]);
     }
     if (nb < 2) return;
-    const uint32_t v2 = __ldg(&N[a]);
+    const uint32_t v2 = N[a];
     const uint64_t e2 = A.eoff[v2];
     const int deg2 = (int)(A.eoff[v2 + 1] - e2);
     const int W2 = (deg2 + 63) >> 6;
@@ -988,7 +988,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
         for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2[k];
     __syncwarp();
     for (int c = a + 1 + lane; c < deg; c += 32) {
-        const uint32_t x = __ldg(&N[c]);
+        const uint32_t x = N[c];
         int lo2 = 0, n2 = deg2;  // lower bound of x in v2's list
         while (n2 > 0) {
             const int h = n2 >> 1;
@@ -1095,6 +1095,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_alpha1(TetArgs A, TetQueue Q, u
     __shared__ uint64_t sL2[8][64];       // v2's link rows (when they fit)
     __shared__ uint32_t sN2[8][kMaxDeg];  // v2's upper neighbours
     __shared__ uint16_t smap[8][64];      // position of N[c] in v2's list, 0xffff: absent
+    __shared__ uint32_t sN[8][64];        // v1's upper neighbours
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
     Tally tally;
@@ -1115,14 +1116,16 @@ __global__ void __launch_bounds__(256, 3) k_tets_alpha1(TetArgs A, TetQueue Q, u
         const uint32_t *N = A.ER + e0;
         const uint64_t *Lp = A.link + A.loff[p];
         for (int c = lane; c < deg; c += 32) {
-            sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
+            const uint32_t x = __ldg(&N[c]);
+            sN[wib][c] = x;
+            sb[wib][c] = __ldg(&A.at[x]);
             sL[wib][c] = Lp[c];
         }
         const Ball B1 = pac::ld_ball(&A.at[p]);
         const MolGrid G = A.grids[mol_of(A.mol, p)];
         __syncwarp();
         for (int a = 0; a < deg - 2; a++)
-            tet_row<V, 1, 64>(A, Q, p, a, deg, 1, N, sL[wib], sb[wib], sN2[wib], sL2[wib],
+            tet_row<V, 1, 64>(A, Q, p, a, deg, 1, sN[wib], sL[wib], sb[wib], sN2[wib], sL2[wib],
                               smap[wib], B1, G, cand_acc, alpha_acc, tally);
         __syncwarp();
     }
@@ -1157,6 +1160,7 @@ __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue 
     __shared__ uint64_t sL2[4][512];  // v2's link rows when they fit (else read in place)
     __shared__ uint32_t sN2[4][kMaxDeg];
     __shared__ uint16_t smap[4][kMaxDeg];
+    __shared__ uint32_t sN[4][kMaxDeg];  // v1's upper neighbours (from the unit's first row)
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
     Tally tally;
@@ -1184,13 +1188,17 @@ __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue 
         const int W = (deg + 63) >> 6;
         const uint32_t *N = A.ER + e0;
         const uint64_t *Lp = A.link + A.loff[p];
-        for (int c = a0 + lane; c < deg; c += 32) sb[wib][c] = __ldg(&A.at[__ldg(&N[c])]);
+        for (int c = a0 + lane; c < deg; c += 32) {
+            const uint32_t x = __ldg(&N[c]);
+            sN[wib][c] = x;
+            sb[wib][c] = __ldg(&A.at[x]);
+        }
         const Ball B1 = pac::ld_ball(&A.at[p]);
         const MolGrid G = A.grids[mol_of(A.mol, p)];
         __syncwarp();
         const int a1 = min(a0 + kUnitRows, deg - 2);
         for (int a = a0; a < a1; a++)
-            tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, N, Lp, sb[wib], sN2[wib], sL2[wib],
+            tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, sN[wib], Lp, sb[wib], sN2[wib], sL2[wib],
                                    smap[wib], B1, G, cand_acc, alpha_acc, tally);
         __syncwarp();
     }
@@ -1206,7 +1214,7 @@ __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue 
 // owns one tetrahedron at a time and evaluates one window ball per step; a
 // warp claims 32 queue entries at a time and a lane takes the next unclaimed
 // one as soon as its own is decided.  A tetrahedron still open after
-// kSerialEvals balls is handed to the cooperative test (the whole warp scans
+// A.handoff balls is handed to the cooperative test (the whole warp scans
 // its window), so no lane runs a long window alone.  Survivors are recorded
 // and mark their faces.
 template <int V>
@@ -1308,7 +1316,7 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             }
             continue;
         }
-        const bool handoff = have && nev >= kSerialEvals;
+        const bool handoff = have && nev >= A.handoff;
         const unsigned hm = __ballot_sync(kFull, handoff);
         if (hm) {
             int pos = ln + __popc(hm & lt_mask);
@@ -2000,6 +2008,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     T.alpha = in.alpha;
     T.ctr = ctr;
     T.gctr = ctr;
+    T.handoff = std::max(1, cfg.handoff);
     T.tcount = ar.alloc_n<uint32_t>(n);
     uint64_t *toff = ar.alloc_n<uint64_t>(n + 1);
     if (!T.tcount || !toff) return PAC_ERR_OOM;
@@ -2104,7 +2113,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             cand_total += ha[C_CAND_Q];
             alpha_total += ha[C_ALPHA_Q];
             CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
-            k_tets_scan<V><<<148 * 4, 256, 0, s>>>(T, Q, queued, claim);
+            k_tets_scan<V><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued, claim);
             LAUNCH_CHECK(ctx);
             // next chunk sized from this one's queue fill
             if (queued)

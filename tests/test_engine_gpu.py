@@ -313,3 +313,15 @@ def test_assembly_2p5m_matches_restatement_digest(pac):
     for k in ("cand_edges", "alpha_edges", "cand_tris", "alpha_tris", "cand_tets", "alpha_tets"):
         assert r.stats[k] == rec["stats"][k], k
     print("2.5M assembly: %.1f ms, %d simplices" % (r.stats["ms_total"], sum(rec["counts"])))
+
+
+def test_autotuner_passes_all_give_the_same_lists(pac, orc):
+    """With autotune on, the first passes of a context each run another
+    launch shape; every pass, tuning or tuned, returns the same lists."""
+    balls = pac.globule(3000, seed=pac.SEED_BASE + 81)
+    e, t, q, _ = orc.alpha_complex(balls, 1.4, 1.0, orc.UPSTREAM, tet_ortho=True)
+    with pac.Engine(autotune=True) as eng:
+        for _ in range(10):  # 8 candidate shapes, then the chosen one
+            _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
+    with pac.Engine(handoff=3, scan_blocks=2) as eng:
+        _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
