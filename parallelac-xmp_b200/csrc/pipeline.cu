@@ -1217,8 +1217,10 @@ __global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue 
 // A.handoff balls is handed to the cooperative test (the whole warp scans
 // its window), so no lane runs a long window alone.  Survivors are recorded
 // and mark their faces.
-template <int V>
-__global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
+// COOP: the cooperative hand-off is compiled in (the autotuner's candidates
+// with a threshold); without it the kernel holds fewer registers.
+template <int V, bool COOP>
+__global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
     __shared__ uint32_t lkey[8][kLongCap];
     __shared__ uint32_t lball[8][kLongCap];
@@ -1310,26 +1312,32 @@ __global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uin
             head = min(tail, head + (uint64_t)__popc(want));
         }
         if (!__any_sync(kFull, have)) {
-            if (!more || ln) {
-                flush_long();
+            if constexpr (COOP) {
+                if (!more || ln) {
+                    flush_long();
+                    if (!more) break;
+                }
+            } else {
                 if (!more) break;
             }
             continue;
         }
-        const bool handoff = have && nev >= A.handoff;
-        const unsigned hm = __ballot_sync(kFull, handoff);
-        if (hm) {
-            int pos = ln + __popc(hm & lt_mask);
-            if (handoff && pos < kLongCap) {
-                lkey[wib][pos] = key;
-                lball[wib][pos] = p;
-                lcell[wib][pos] = mycell;
-                have = false;
-            }
-            ln = min(kLongCap, ln + __popc(hm));
-            if (ln > kLongCap - 32) {
-                __syncwarp();
-                flush_long();
+        if constexpr (COOP) {
+            const bool handoff = have && nev >= A.handoff;
+            const unsigned hm = __ballot_sync(kFull, handoff);
+            if (hm) {
+                int pos = ln + __popc(hm & lt_mask);
+                if (handoff && pos < kLongCap) {
+                    lkey[wib][pos] = key;
+                    lball[wib][pos] = p;
+                    lcell[wib][pos] = mycell;
+                    have = false;
+                }
+                ln = min(kLongCap, ln + __popc(hm));
+                if (ln > kLongCap - 32) {
+                    __syncwarp();
+                    flush_long();
+                }
             }
         }
         if (!have) continue;
@@ -2113,7 +2121,12 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             cand_total += ha[C_CAND_Q];
             alpha_total += ha[C_ALPHA_Q];
             CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
-            k_tets_scan<V><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued, claim);
+            if (cfg.handoff < (1 << 30))
+                k_tets_scan<V, true><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued,
+                                                                                     claim);
+            else
+                k_tets_scan<V, false><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued,
+                                                                                      claim);
             LAUNCH_CHECK(ctx);
             // next chunk sized from this one's queue fill
             if (queued)
