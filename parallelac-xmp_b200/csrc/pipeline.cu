@@ -1088,7 +1088,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
 // the chunk [lo, hi).  The balls of v1's neighbours and v1's link rows are
 // staged in shared memory once per ball.
 template <int V>
-__global__ void __launch_bounds__(256, 3) k_tets_alpha1(TetArgs A, TetQueue Q, uint64_t lo,
+__global__ void __launch_bounds__(256, 4) k_tets_alpha1(TetArgs A, TetQueue Q, uint64_t lo,
                                                         uint64_t hi) {
     __shared__ float4 sb[8][64];          // balls of v1's upper neighbours
     __shared__ uint64_t sL[8][64];        // v1's link rows
@@ -1154,7 +1154,7 @@ __global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, uint32_t *rows) {
 // handed out from a counter.  Per unit the balls of v1's neighbours beyond
 // its first row are staged.
 template <int V>
-__global__ void __launch_bounds__(128, 4) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
+__global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
                                                             uint64_t hi, const uint64_t *uoff) {
     __shared__ float4 sb[4][kMaxDeg];
     __shared__ uint64_t sL2[4][512];  // v2's link rows when they fit (else read in place)
@@ -1551,7 +1551,7 @@ __global__ void k_map4(uint64_t nq, const uint32_t *orig, uint32_t *tets) {
 constexpr int kTQCap = 256;
 
 template <int V>
-__global__ void __launch_bounds__(256, 3) k_tri_attach(uint64_t n, const float4 *__restrict__ at,
+__global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t n, const float4 *__restrict__ at,
                                                        const uint64_t *__restrict__ eoff,
                                                        const uint32_t *__restrict__ ER,
                                                        const uint64_t *__restrict__ loff,
@@ -2076,12 +2076,12 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             TetArgs TA = T;
             TA.ctr = ctrA;
             CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
-            k_tets_alpha1<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 3), 256, 0, s>>>(
+            k_tets_alpha1<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 4), 256, 0, s>>>(
                 TA, Q, lo, hi);
             LAUNCH_CHECK(ctx);
             if (heavy_units) {  // balls with more than 64 upper neighbours, by rows
                 CK(cudaMemsetAsync(ctrA + C_NEXT, 0, sizeof(unsigned long long), s));
-                k_tets_alpha_rows<V><<<148 * 4, 128, 0, s>>>(TA, Q, lo, hi, uoff);
+                k_tets_alpha_rows<V><<<148 * 6, 128, 0, s>>>(TA, Q, lo, hi, uoff);
                 LAUNCH_CHECK(ctx);
             }
             unsigned long long ha[C_NCOUNTERS], used[2];
@@ -2171,7 +2171,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
     if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
     CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
-    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(n), 148 * 3), 256, 0, s>>>(
+    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(n), 148 * 4), 256, 0, s>>>(
         n, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids, in.alpha, ctr);
     LAUNCH_CHECK(ctx);
     tm.mark();  // 5
