@@ -581,6 +581,7 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
                                               const uint64_t *__restrict__ loff, uint64_t *link,
                                               float alpha, unsigned long long *ctr) {
     __shared__ uint64_t srow[8][kMaxW];
+    __shared__ uint64_t sL[8][64];  // link rows of a ball of <= 64 upper neighbours
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -594,6 +595,46 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
         const uint32_t *N = ER + e0;
         uint64_t *L = link + loff[p];
         const Ball A = pac::ld_ball(&at[p]);
+        if (deg <= 64) {
+            // all pairs (a, b), a < b, flattened over the lanes: row a holds
+            // deg - 1 - a of them, P(a) = a (2 deg - 1 - a) / 2 before it
+            const int total = deg * (deg - 1) / 2;
+            for (int k = lane; k < deg; k += 32) sL[wib][k] = 0;
+            __syncwarp();
+            for (int base = 0; base < total; base += 32) {
+                const int s2 = base + lane;
+                bool cand = false, pass = false;
+                int a = 0, b = 0;
+                if (s2 < total) {
+                    const float D = (float)(2 * deg - 1);
+                    a = (int)((D - sqrtf(D * D - 8.0f * (float)s2)) * 0.5f);
+                    a = max(0, min(a, deg - 2));
+                    while (a > 0 && a * (2 * deg - 1 - a) / 2 > s2) a--;
+                    while (a + 1 <= deg - 2 && (a + 1) * (2 * deg - 2 - a) / 2 <= s2) a++;
+                    b = a + 1 + (s2 - a * (2 * deg - 1 - a) / 2);
+                    const uint32_t v1 = __ldg(&N[a]), v2 = __ldg(&N[b]);
+                    const uint64_t e1 = eoff[v1];
+                    const int deg1 = (int)(eoff[v1 + 1] - e1);
+                    const int pos = lbound(ER + e1, deg1, v2);
+                    cand = pos < deg1 && __ldg(&ER[e1 + pos]) == v2;
+                    if (cand) {
+                        float4 o;
+                        pass = dec_tri<V>(A, pac::ld_ball(&at[v1]), pac::ld_ball(&at[v2]), alpha, o,
+                                          tally);
+                    }
+                    if (pass) atomicOr((unsigned long long *)&sL[wib][a], 1ull << b);
+                }
+                const unsigned cm = __ballot_sync(kFull, cand), pm = __ballot_sync(kFull, pass);
+                if (lane == 0) {
+                    cand_acc += __popc(cm);
+                    alpha_acc += __popc(pm);
+                }
+            }
+            __syncwarp();
+            for (int k = lane; k < deg; k += 32) L[k] = sL[wib][k];
+            __syncwarp();
+            continue;
+        }
         for (int a = 0; a < deg - 1; a++) {
             if (lane < kMaxW) srow[wib][lane] = 0;
             __syncwarp();
