@@ -922,6 +922,10 @@ __device__ __forceinline__ void window_centre(const MolGrid &G, const uint32_t *
 }
 
 constexpr int kLongCap = 64;   // tetrahedra handed to the cooperative scan
+// Queue entries a warp of k_tets_scan claims at a time: one counter serves
+// every warp, and claims of 32 made the atomics a bottleneck (25.6 ms for
+// the stage at 100k balls; 24.4 with 128, 24.2 with 512).
+constexpr uint64_t kScanClaim = 512;
 
 // Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
 // lane 0 owns the centre cell, lanes 1..10 the window's other parts, and a
@@ -1252,14 +1256,13 @@ __global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue 
 
 // k_tets_scan: the empty-orthosphere test (checkTetsOrthosphere,
 // AlphaComplexLargeData.cu:606-734) of the queued tetrahedra.  Each lane
-// owns one tetrahedron at a time and evaluates one window ball per step; a
-// warp claims 32 queue entries at a time and a lane takes the next unclaimed
-// one as soon as its own is decided.  A tetrahedron still open after
-// A.handoff balls is handed to the cooperative test (the whole warp scans
-// its window), so no lane runs a long window alone.  Survivors are recorded
-// and mark their faces.
-// COOP: the cooperative hand-off is compiled in (the autotuner's candidates
-// with a threshold); without it the kernel holds fewer registers.
+// owns one tetrahedron at a time and evaluates two window balls per step; a
+// warp claims kScanClaim queue entries at a time and a lane takes the next
+// unclaimed one as soon as its own is decided.  Survivors are recorded and
+// mark their faces.  COOP (the autotuner's candidates with a hand-off
+// threshold): a tetrahedron still open after A.handoff balls is handed to
+// the cooperative test (the whole warp scans its window); without it the
+// kernel holds fewer registers and runs four blocks per SM.
 template <int V, bool COOP>
 __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
@@ -1314,10 +1317,10 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
         unsigned want = __ballot_sync(kFull, !have);
         if (want && head >= tail && more) {
             uint64_t b = 0;
-            if (lane == 0) b = atomicAdd(claim, 32ull);
+            if (lane == 0) b = atomicAdd(claim, (unsigned long long)kScanClaim);
             b = __shfl_sync(kFull, b, 0);
             head = b;
-            tail = min(nq, b + 32);
+            tail = min(nq, b + kScanClaim);
             if (head >= tail) more = false;
         }
         if (want && head < tail) {
