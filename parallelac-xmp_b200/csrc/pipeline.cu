@@ -2115,10 +2115,15 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         }
         unsigned long long cand_total = 0, alpha_total = 0;
         uint64_t lo = 0, chunk = n;
+        // verbose: per-chunk enumeration and scan times
+        cudaEvent_t vev[3] = {nullptr, nullptr, nullptr};
+        if (cfg.verbose)
+            for (auto &e : vev) CK(cudaEventCreate(&e));
         while (lo < n) {
             const uint64_t hi = std::min<uint64_t>(n, lo + chunk);
             TetArgs TA = T;
             TA.ctr = ctrA;
+            if (cfg.verbose) CK(cudaEventRecord(vev[0], s));
             CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
             k_tets_alpha1<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 4), 256, 0, s>>>(
                 TA, Q, lo, hi);
@@ -2128,6 +2133,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                 k_tets_alpha_rows<V><<<148 * 6, 128, 0, s>>>(TA, Q, lo, hi, uoff);
                 LAUNCH_CHECK(ctx);
             }
+            if (cfg.verbose) CK(cudaEventRecord(vev[1], s));
             unsigned long long ha[C_NCOUNTERS], used[2];
             CK(cudaMemcpyAsync(ha, ctrA, sizeof(ha), cudaMemcpyDeviceToHost, s));
             CK(cudaMemcpyAsync(used, ctr + C_SURV, sizeof(used), cudaMemcpyDeviceToHost, s));
@@ -2172,6 +2178,18 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                 k_tets_scan<V, false><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued,
                                                                                       claim);
             LAUNCH_CHECK(ctx);
+            if (cfg.verbose) {
+                float me = 0.f, ms = 0.f;
+                CK(cudaEventRecord(vev[2], s));
+                CK(cudaEventSynchronize(vev[2]));
+                CK(cudaEventElapsedTime(&me, vev[0], vev[1]));
+                CK(cudaEventElapsedTime(&ms, vev[1], vev[2]));
+                std::fprintf(stderr,
+                             "[pac] tetrahedra of balls [%llu, %llu): %llu candidates, %llu alpha, "
+                             "%llu queued; enumeration %.3f ms, scan %.3f ms\n",
+                             (unsigned long long)lo, (unsigned long long)hi, ha[C_CAND_Q],
+                             ha[C_ALPHA_Q], queued, me, ms);
+            }
             // next chunk sized from this one's queue fill
             if (queued)
                 chunk = std::max<uint64_t>(
@@ -2180,6 +2198,8 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                 chunk = n;
             lo = hi;
         }
+        if (cfg.verbose)
+            for (auto &e : vev) cudaEventDestroy(e);
         {
             unsigned long long cq[2] = {cand_total, alpha_total};
             CK(cudaMemcpyAsync(ctr + C_CAND_Q, cq, sizeof(cq), cudaMemcpyHostToDevice, s));
@@ -2328,6 +2348,12 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             st->step = hg[0].step;
         }
     }
+    if (cfg.verbose)
+        std::fprintf(stderr,
+                     "[pac] %llu balls: grid %.3f, edges %.3f, triangles %.3f, tetrahedra %.3f, "
+                     "triangle attachment %.3f, edge attachment %.3f, emission %.3f ms\n",
+                     (unsigned long long)n, tm.ms(0, 1), tm.ms(1, 2), tm.ms(2, 3), tm.ms(3, 4),
+                     tm.ms(4, 5), tm.ms(5, 6), tm.ms(6, 7));
     return PAC_OK;
 }
 
