@@ -291,6 +291,20 @@ def test_chunked_tetrahedron_queue(pac, orc):
     assert r.stats["alpha_tets"] == st["alpha_tets"] and r.stats["cand_tets"] == st["cand_tets"]
 
 
+def test_verbose_reports_chunks_and_stages(pac, capfd):
+    """verbose: one line per tetrahedron chunk (its counts add up to the
+    pass's) and one line of stage timings per pass, on stderr."""
+    balls = pac.globule(4000, seed=pac.SEED_BASE + 12)
+    with pac.Engine(tet_mode="as-written", queue_entries=200_000, verbose=True) as eng:
+        r = eng.alpha_complex(balls, 1.4, 1.0)
+    err = capfd.readouterr().err
+    chunks = [l for l in err.splitlines() if l.startswith("[pac] tetrahedra of balls")]
+    assert len(chunks) > 1
+    alpha = sum(int(l.split(": ")[1].split(", ")[1].split()[0]) for l in chunks)
+    assert alpha == r.stats["alpha_tets"]
+    assert any(l.startswith("[pac] %d balls: grid" % len(balls)) for l in err.splitlines())
+
+
 @pytest.mark.slow
 def test_assembly_2p5m_matches_restatement_digest(pac):
     """The north star's large single pass: 2.5M balls (400 globules of 6,250
