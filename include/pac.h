@@ -120,7 +120,7 @@ typedef struct {
     int reserved_i[9];
     /* reserved_u[0]: if nonzero, the number of alpha tetrahedra the pass
        queues per chunk (default: a quarter of free device memory, at most
-       8 GiB, 24 B per entry).  Smaller values force more chunks. */
+       12 GiB, 32 B per entry).  Smaller values force more chunks. */
     uint64_t reserved_u[8];
 } pac_options;
 

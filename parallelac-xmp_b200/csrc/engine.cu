@@ -121,16 +121,16 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
         return pac::set_error(PAC_ERR_CUDA, std::string("input check: ") + cudaGetErrorString(e));
     if (hbad) return pac::set_error(PAC_ERR_INVALID_ARG, "non-finite ball coordinate or radius");
     // the alpha-tetrahedron queue: a quarter of the free memory at the
-    // context's first pass, at most 8 GiB (24 B per entry); a pass larger
+    // context's first pass, at most 12 GiB (32 B per entry); a pass larger
     // than that runs in chunks
     if (!c.queue_bytes) {
         size_t freeb = 0, totalb = 0;
         cudaMemGetInfo(&freeb, &totalb);
-        c.queue_bytes = std::max<uint64_t>(std::min<uint64_t>(freeb / 4, 8ull << 30), 24ull << 16);
+        c.queue_bytes = std::max<uint64_t>(std::min<uint64_t>(freeb / 4, 12ull << 30), 32ull << 16);
     }
     uint64_t qbytes = c.queue_bytes;
-    if (c.opt.reserved_u[0]) qbytes = c.opt.reserved_u[0] * 24ull;  // test hook: entries
-    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 24,
+    if (c.opt.reserved_u[0]) qbytes = c.opt.reserved_u[0] * 32ull;  // test hook: entries
+    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 32,
                             c.opt.predicates == PAC_PRED_EXACT, kShapes[0].handoff,
                             kShapes[0].scan_blocks};
     // launch shapes: the caller's overrides, else the autotuner's current

@@ -840,6 +840,14 @@ __global__ void __launch_bounds__(256) k_tets(TetArgs A) {
     }
 }
 
+// Positions of v2 < v3 < v4 in ball p's upper-neighbour list N (ascending,
+// deg entries), packed a | b << 8 | c << 16 as the survivor lists hold them.
+__device__ __forceinline__ uint32_t key_of(const uint32_t *N, int deg, uint32_t v2, uint32_t v3,
+                                           uint32_t v4) {
+    return (uint32_t)lbound(N, deg, v2) | ((uint32_t)lbound(N, deg, v3) << 8) |
+           ((uint32_t)lbound(N, deg, v4) << 16);
+}
+
 __device__ __noinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
                                               const uint32_t *N, uint32_t key, bool pending,
                                               uint32_t &ball_count) {
@@ -994,7 +1002,7 @@ __device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32
 // candidate, and the passing tetrahedra are appended to the queue with the
 // cell of their orthosphere centre.
 struct TetQueue {
-    uint2 *pk;        // (ball v1, a | b << 8 | c << 16)
+    uint4 *vid;       // (v1, v2, v3, v4): the scan loads the balls directly
     int4 *cell;       // (gridX, gridY, gridZ, linear centre index)
     uint64_t cap;
 };
@@ -1114,8 +1122,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
             if (passA) {
                 uint64_t pos = qbase + __popc(mA & lt_mask);
                 if (pos < Q.cap) {
-                    Q.pk[pos] = make_uint2((uint32_t)p,
-                                           (uint32_t)a | ((uint32_t)bo << 8) | ((uint32_t)c << 16));
+                    Q.vid[pos] = make_uint4((uint32_t)p, v2, N[bo], N[c]);
                     Q.cell[pos] = cell;
                 }
             }
@@ -1266,8 +1273,7 @@ __global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue 
 template <int V, bool COOP>
 __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
-    __shared__ uint32_t lkey[8][kLongCap];
-    __shared__ uint32_t lball[8][kLongCap];
+    __shared__ uint4 lvid[8][kLongCap];
     __shared__ int4 lcell[8][kLongCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1;
@@ -1275,7 +1281,7 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
     Tally tally;
     uint64_t head = 0, tail = 0;  // this warp's claimed range (warp-uniform)
     bool have = false, more = true;
-    uint32_t p = 0, key = 0, v2 = 0, v3 = 0, v4 = 0;
+    uint32_t p = 0, v2 = 0, v3 = 0, v4 = 0;
     float pa[3], pb[3], pc[3], pd[3], wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
     int gX = 0, gY = 0, gZ = 0, q = 0, nev = 0;
     int4 mycell = make_int4(0, 0, 0, 0);
@@ -1285,11 +1291,9 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
     const MolGrid *G = A.grids;
     auto flush_long = [&]() {
         for (int t = 0; t < ln; t++) {
-            const uint32_t k2 = lkey[wib][t], p2 = lball[wib][t];
+            const uint4 vv = lvid[wib][t];
+            const uint32_t p2 = vv.x, u2 = vv.y, u3 = vv.z, u4 = vv.w;
             const int4 cl = lcell[wib][t];
-            const uint32_t *N2 = A.ER + A.eoff[p2];
-            const uint32_t u2 = __ldg(&N2[k2 & 0xff]), u3 = __ldg(&N2[(k2 >> 8) & 0xff]),
-                           u4 = __ldg(&N2[(k2 >> 16) & 0xff]);
             const Ball a1 = pac::ld_ball(&A.at[p2]), a2 = pac::ld_ball(&A.at[u2]),
                        a3 = pac::ld_ball(&A.at[u3]), a4 = pac::ld_ball(&A.at[u4]);
             float qa[3], qb[3], qc[3], qd[3];
@@ -1303,9 +1307,11 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
             int r = coop_test<V>(A, G2, p2, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc, xd, ori, cl, evals,
                                  tally);
             if (r != 1 && lane == 0) {
+                const uint32_t *N2 = A.ER + A.eoff[p2];
                 const int deg = (int)(A.eoff[p2 + 1] - A.eoff[p2]);
                 uint32_t dummy = 0;
-                emit_survivor(A, p2, (deg + 63) >> 6, A.loff[p2], N2, k2, r == 2, dummy);
+                emit_survivor(A, p2, (deg + 63) >> 6, A.loff[p2], N2, key_of(N2, deg, u2, u3, u4),
+                              r == 2, dummy);
                 if (r != 2) atomicAdd(&A.tcount[p2], 1u);
             }
         }
@@ -1327,15 +1333,13 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
             int r = __popc(want & lt_mask);
             if (!have && head + r < tail) {
                 uint64_t idx = head + r;
-                uint2 pk = Q.pk[idx];
+                const uint4 vv = Q.vid[idx];
                 int4 cl = Q.cell[idx];
-                p = pk.x;
-                key = pk.y;
+                p = vv.x;
+                v2 = vv.y;
+                v3 = vv.z;
+                v4 = vv.w;
                 G = A.grids + mol_of(A.mol, p);
-                const uint32_t *N = A.ER + A.eoff[p];
-                v2 = __ldg(&N[key & 0xff]);
-                v3 = __ldg(&N[(key >> 8) & 0xff]);
-                v4 = __ldg(&N[(key >> 16) & 0xff]);
                 const Ball a1 = pac::ld_ball(&A.at[p]), a2 = pac::ld_ball(&A.at[v2]),
                            a3 = pac::ld_ball(&A.at[v3]), a4 = pac::ld_ball(&A.at[v4]);
                 pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = wt<V>(a1.r);
@@ -1372,8 +1376,7 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
             if (hm) {
                 int pos = ln + __popc(hm & lt_mask);
                 if (handoff && pos < kLongCap) {
-                    lkey[wib][pos] = key;
-                    lball[wib][pos] = p;
+                    lvid[wib][pos] = make_uint4(p, v2, v3, v4);
                     lcell[wib][pos] = mycell;
                     have = false;
                 }
@@ -1434,7 +1437,8 @@ __global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQ
             const uint32_t *N = A.ER + A.eoff[p];
             const int deg = (int)(A.eoff[p + 1] - A.eoff[p]);
             uint32_t dummy = 0;
-            emit_survivor(A, p, (deg + 63) >> 6, A.loff[p], N, key, zero, dummy);
+            emit_survivor(A, p, (deg + 63) >> 6, A.loff[p], N, key_of(N, deg, v2, v3, v4), zero,
+                          dummy);
             if (!zero) atomicAdd(&A.tcount[p], 1u);
             have = false;
         }
@@ -2085,7 +2089,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         // queue of alpha tetrahedra in HBM, processed in chunks of balls
         const uint64_t qcap = std::max<uint64_t>(1 << 16, cfg.queue_entries);
         TetQueue Q;
-        Q.pk = ar.alloc_n<uint2>(qcap);
+        Q.vid = ar.alloc_n<uint4>(qcap);
         Q.cell = ar.alloc_n<int4>(qcap);
         Q.cap = qcap;
         uint64_t scap = std::max<uint64_t>(1024, 16 * n);
@@ -2095,7 +2099,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         T.pend_cap = scap / 4 + 1024;
         unsigned long long *claim = ar.alloc_n<unsigned long long>(1);
         unsigned long long *ctrA = ar.alloc_n<unsigned long long>(C_NCOUNTERS);
-        if (!Q.pk || !Q.cell || !T.surv || !T.pend || !claim || !ctrA) return PAC_ERR_OOM;
+        if (!Q.vid || !Q.cell || !T.surv || !T.pend || !claim || !ctrA) return PAC_ERR_OOM;
         CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
