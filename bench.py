@@ -138,7 +138,8 @@ REF_WARM = 1_300
 
 
 def config_of(n):
-    return {"workload": "100k-ball globule (0.05/A^3) + 8 isolated corner balls, sol 1.4, "
+    size = "100k" if n - 8 == N_BALLS else "%d" % (n - 8)
+    return {"workload": size + "-ball globule (0.05/A^3) + 8 isolated corner balls, sol 1.4, "
                         "alpha 1.0, upstream formulas, orthosphere test applied, strict f32",
             "n_balls": n, "sol_rad": SOL, "alpha": ALPHA, "parallelism": "dp1",
             "l2": "flushed between steps (256 MB write)"}
