@@ -72,6 +72,10 @@ def build(verbose=False, ptxas_info=False):
         (os.path.join(OBJ, "engine.o"),
          [NVCC] + NVFLAGS + extra + ["-c", os.path.join(SRC, "engine.cu")],
          [os.path.join(SRC, "engine.cu")] + hdrs),
+        (os.path.join(OBJ, "textio.o"),
+         [HOSTCC, "-O2", "-std=c++17", "-fPIC", "-pthread", "-I", INC, "-c",
+          os.path.join(SRC, "textio.cpp")],
+         [os.path.join(SRC, "textio.cpp"), os.path.join(INC, "pac.h")]),
     ]
     todo = [(o, c + ["-o", o]) for o, c, deps in jobs if _stale(o, deps)]
     logs = []
@@ -81,7 +85,8 @@ def build(verbose=False, ptxas_info=False):
     objs = [o for o, _, _ in jobs]
     lib = os.path.join(LIB, "libpac.so")
     if _stale(lib, objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-ccbin", HOSTCC, "-o", lib] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-ccbin", HOSTCC, "-o", lib] + objs +
+             ["-lpthread"])
     synth = os.path.join(LIB, "libpac_synth.so")
     if _stale(synth, [os.path.join(SRC, "synth.c")]):
         _run([HOSTC, "-O2", "-std=c99", "-fPIC", "-shared", "-o", synth,

@@ -590,76 +590,6 @@ const char *pac_status_string(int status) {
 
 const char *pac_last_error(void) { return pac::g_last_error.c_str(); }
 
-// CRD input: the reference reads the count with "%d" and each ball with
-// "%f %f %f %f" (AlphaComplexLargeData.cu:1070, 1079); strtof gives the same
-// correctly rounded floats.
-int pac_read_crd(const char *path, pac_ball **balls, uint32_t *n) {
-    if (!path || !balls || !n) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
-    *balls = nullptr;
-    *n = 0;
-    FILE *f = std::fopen(path, "rb");
-    if (!f) return pac::set_error(PAC_ERR_IO, std::string("cannot open ") + path);
-    std::fseek(f, 0, SEEK_END);
-    long sz = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    std::vector<char> buf((size_t)std::max(sz, 0L) + 1);
-    size_t got = std::fread(buf.data(), 1, (size_t)std::max(sz, 0L), f);
-    std::fclose(f);
-    buf[got] = 0;
-    char *p = buf.data(), *end = nullptr;
-    errno = 0;
-    long cnt = std::strtol(p, &end, 10);
-    if (end == p || cnt < 0 || cnt > 0xfffffffeL)
-        return pac::set_error(PAC_ERR_IO, std::string("bad ball count in ") + path);
-    p = end;
-    pac_ball *b = (pac_ball *)std::malloc(sizeof(pac_ball) * (size_t)(cnt ? cnt : 1));
-    if (!b) return pac::set_error(PAC_ERR_OOM, "host allocation failed");
-    for (long i = 0; i < cnt; i++) {
-        float v[4];
-        for (int k = 0; k < 4; k++) {
-            v[k] = std::strtof(p, &end);
-            if (end == p) {
-                std::free(b);
-                return pac::set_error(PAC_ERR_IO, std::string(path) + ": ball " +
-                                                      std::to_string(i) + " is truncated");
-            }
-            p = end;
-        }
-        b[i] = pac_ball{v[0], v[1], v[2], v[3]};
-    }
-    *balls = b;
-    *n = (uint32_t)cnt;
-    return PAC_OK;
-}
-
-// The reference's output file (AlphaComplexLargeData.cu:2028-2050).
-int pac_write_complex(const char *path, const pac_ball *balls, uint32_t n, float sol_rad,
-                      const pac_complex *cx) {
-    if (!path || !cx || (n && !balls)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
-    if (cx->on_device == 1)
-        return pac::set_error(PAC_ERR_INVALID_ARG, "complex lists are in device memory");
-    FILE *fp = std::fopen(path, "w");
-    if (!fp) return pac::set_error(PAC_ERR_IO, std::string("cannot create ") + path);
-    std::vector<char> obuf(1 << 20);
-    std::setvbuf(fp, obuf.data(), _IOFBF, obuf.size());
-    std::fprintf(fp, "%d %ld %ld %ld\n", (int)n, (long)cx->n_edges, (long)cx->n_tris,
-                 (long)cx->n_tets);
-    for (uint32_t i = 0; i < n; i++) {
-        float r = balls[i].r + sol_rad;
-        std::fprintf(fp, "%9.5lf %9.5lf %9.5lf %9.5lf\n", (double)balls[i].x, (double)balls[i].y,
-                     (double)balls[i].z, (double)r);
-    }
-    for (uint64_t i = 0; i < cx->n_edges; i++)
-        std::fprintf(fp, "%9d %9d\n", (int)cx->edges[2 * i], (int)cx->edges[2 * i + 1]);
-    for (uint64_t i = 0; i < cx->n_tris; i++)
-        std::fprintf(fp, "%9d %9d %9d\n", (int)cx->tris[3 * i], (int)cx->tris[3 * i + 1],
-                     (int)cx->tris[3 * i + 2]);
-    for (uint64_t i = 0; i < cx->n_tets; i++)
-        std::fprintf(fp, "%9d %9d %9d %9d\n", (int)cx->tets[4 * i], (int)cx->tets[4 * i + 1],
-                     (int)cx->tets[4 * i + 2], (int)cx->tets[4 * i + 3]);
-    int bad = std::ferror(fp);
-    if (std::fclose(fp) != 0 || bad) return pac::set_error(PAC_ERR_IO, std::string("write failed: ") + path);
-    return PAC_OK;
-}
+// pac_read_crd and pac_write_complex: textio.cpp.
 
 }  // extern "C"
