@@ -14,6 +14,7 @@ CUDA device is missing, the calls raise.
 """
 import ctypes
 import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -134,10 +135,24 @@ def _check(status):
         raise PacError(status, _lib().pac_last_error().decode())
 
 
+def _copy(src):
+    """Copy of a large array, in slices on several threads (numpy releases
+    the GIL while copying): lists of a batched pass run to gigabytes."""
+    if src.nbytes < (16 << 20):
+        return src.copy()
+    out = np.empty_like(src)
+    parts = min(16, os.cpu_count() or 1)
+    step = -(-len(src) // parts)
+    with ThreadPoolExecutor(parts) as ex:
+        list(ex.map(lambda i: np.copyto(out[i * step:(i + 1) * step], src[i * step:(i + 1) * step]),
+                    range(parts)))
+    return out
+
+
 def _arr(ptr, count, k):
     if count == 0:
         return np.zeros((0, k), np.uint32)
-    return np.ctypeslib.as_array(ptr, (count * k,)).reshape(count, k).copy()
+    return _copy(np.ctypeslib.as_array(ptr, (count * k,))).reshape(count, k)
 
 
 class Result:
