@@ -1209,7 +1209,7 @@ template <int V>
 __global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
                                                             uint64_t hi, const uint64_t *uoff) {
     __shared__ float4 sb[4][kMaxDeg];
-    __shared__ uint64_t sL2[4][512];  // v2's link rows when they fit (else read in place)
+    __shared__ uint64_t sL2[4][256];  // v2's link rows when they fit (else read in place)
     __shared__ uint32_t sN2[4][kMaxDeg];
     __shared__ uint16_t smap[4][kMaxDeg];
     __shared__ uint32_t sN[4][kMaxDeg];  // v1's upper neighbours (from the unit's first row)
@@ -1250,7 +1250,7 @@ __global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue 
         __syncwarp();
         const int a1 = min(a0 + kUnitRows, deg - 2);
         for (int a = a0; a < a1; a++)
-            tet_row<V, kMaxW, 512>(A, Q, p, a, deg, W, sN[wib], Lp, sb[wib], sN2[wib], sL2[wib],
+            tet_row<V, kMaxW, 256>(A, Q, p, a, deg, W, sN[wib], Lp, sb[wib], sN2[wib], sL2[wib],
                                    smap[wib], B1, G, cand_acc, alpha_acc, tally);
         __syncwarp();
     }
