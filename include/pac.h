@@ -112,7 +112,8 @@ typedef struct {
        stage; later passes use the fastest.  Every shape gives the same
        lists, so tuning passes return correct results too. */
     int autotune;
-    int verbose;     /* 1: print per-stage timings to stderr */
+    int verbose;     /* 1: print per-stage timings of each pass and, per chunk of
+                        the tetrahedron stage, its counts and times to stderr */
     /* reserved_i[0]: if > 0, the scan's hand-off threshold (window balls a
        lane tests alone before the whole warp takes the tetrahedron; default:
        never); reserved_i[1]: if > 0, the scan's blocks per SM (default 4).

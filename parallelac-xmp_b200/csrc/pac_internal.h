@@ -40,7 +40,7 @@ struct PipelineConfig {
     int formula;    // pac_formula
     int tet_mode;   // pac_tet_mode
     int verbose;
-    uint64_t queue_entries;  // alpha tetrahedra queued per chunk (24 B each)
+    uint64_t queue_entries;  // alpha tetrahedra queued per chunk (32 B each)
     bool exact;              // decision-exact predicates (strict flavour only)
     // launch shapes (the output does not depend on them)
     int handoff;      // window balls a scan lane tests alone before the warp takes over
@@ -86,7 +86,7 @@ struct Ctx {
     void *pinned = nullptr;
     size_t pinned_size = 0;
     // bytes for the alpha-tetrahedron queue, fixed at the context's first
-    // pass (a quarter of the memory free then, at most 8 GiB), so that later
+    // pass (a quarter of the memory free then, at most 12 GiB), so that later
     // passes lay out the pool the same way
     uint64_t queue_bytes = 0;
     Tuner tuner;
