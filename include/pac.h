@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PAC_ABI_VERSION 1
+#define PAC_ABI_VERSION 2
 
 typedef enum {
     PAC_OK = 0,
@@ -107,17 +107,25 @@ typedef struct {
     int predicates;  /* pac_pred_mode, default PAC_PRED_REFCOMPAT */
     int order;       /* pac_order, default PAC_ORDER_REFERENCE */
     /* 1: pick launch shapes by measurement.  The context's first passes
-       each try one candidate shape (the orthosphere scan's hand-off
-       threshold and blocks per SM; 8 candidates), timing the tetrahedron
-       stage; later passes use the fastest.  Every shape gives the same
-       lists, so tuning passes return correct results too. */
+       each try one candidate shape (blocks per SM of the tetrahedron
+       enumeration and scan kernels, rows of a large ball per enumeration
+       work unit, queue entries a scan warp claims; 12 candidates), timing
+       the tetrahedron stage; later passes use the fastest.  Every shape
+       gives the same lists, so tuning passes return correct results too. */
     int autotune;
     int verbose;     /* 1: print per-stage timings of each pass and, per chunk of
                         the tetrahedron stage, its counts and times to stderr */
-    /* reserved_i[0]: if > 0, the scan's hand-off threshold (window balls a
-       lane tests alone before the whole warp takes the tetrahedron; default:
-       never); reserved_i[1]: if > 0, the scan's blocks per SM (default 4).
-       Either one turns the autotuner off. */
+    /* Launch-shape overrides, each used when > 0 (any of them turns the
+       autotuner off): reserved_i[0] blocks per SM of the enumeration of
+       balls with at most 64 upper neighbours (default 4), [1] of the
+       orthosphere scan (4), [2] of the enumeration of larger balls (4),
+       [3] rows of a large ball per work unit (8), [4] queue entries a scan
+       warp claims (512).
+       reserved_i[5] = 1: no early refutation in the enumeration (every
+       alpha tetrahedron goes to the scan; same lists).
+       reserved_i[6] = 1: verify mode -- the scan also replays the
+       reference's arithmetic for every decision the certified filter takes
+       and counts disagreements (pac_stats.cert_disagreements; 0 expected). */
     int reserved_i[9];
     /* reserved_u[0]: if nonzero, the number of alpha tetrahedra the pass
        queues per chunk (default: a quarter of free device memory, at most
@@ -175,6 +183,13 @@ typedef struct {
     uint32_t grid[3];
     float step;
     uint32_t kernels_launched;
+    /* as-written tetrahedra (ABI version 2): alpha tetrahedra refuted inside
+       the enumeration by the best other candidate of their triangle group,
+       and the tests made there; orthosphere-scan decisions taken by the
+       certified filter (the rest replay the reference's arithmetic), and in
+       verify mode the certified decisions the replay disagrees with */
+    uint64_t early_refuted, early_tests;
+    uint64_t cert_decisions, cert_disagreements;
 } pac_stats;
 
 /* Version of this ABI (PAC_ABI_VERSION). */

@@ -65,6 +65,7 @@ _STAT_U64 = ["n_balls", "n_cells", "cand_edges", "alpha_edges", "cand_tris", "al
              "cand_tets", "alpha_tets", "final_edges", "final_tris", "final_tets",
              "insphere_evals", "sos_calls", "exact_fallbacks", "filter_evals",
              "ortho_out_of_grid", "max_degree"]
+_STAT_U64B = ["early_refuted", "early_tests", "cert_decisions", "cert_disagreements"]
 _STAT_F64 = ["ms_total", "ms_h2d", "ms_grid", "ms_edges", "ms_tris", "ms_tets",
              "ms_tri_attach", "ms_edge_attach", "ms_emit", "ms_d2h"]
 
@@ -73,7 +74,8 @@ class Stats(ctypes.Structure):
     _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] +
                 [(k, ctypes.c_double) for k in _STAT_F64] +
                 [("bytes_model", ctypes.c_uint64), ("grid", ctypes.c_uint32 * 3),
-                 ("step", ctypes.c_float), ("kernels_launched", ctypes.c_uint32)])
+                 ("step", ctypes.c_float), ("kernels_launched", ctypes.c_uint32)] +
+                [(k, ctypes.c_uint64) for k in _STAT_U64B])
 
     def as_dict(self):
         d = {k: int(getattr(self, k)) for k in _STAT_U64}
@@ -82,6 +84,7 @@ class Stats(ctypes.Structure):
         d["grid"] = list(self.grid)
         d["step"] = float(self.step)
         d["kernels_launched"] = int(self.kernels_launched)
+        d.update({k: int(getattr(self, k)) for k in _STAT_U64B})
         return d
 
 
@@ -171,8 +174,11 @@ class Engine:
 
     def __init__(self, device=0, formula="upstream", tet_mode="as-written", predicates="strict",
                  order="reference", verbose=False, queue_entries=None, autotune=False,
-                 handoff=None, scan_blocks=None):
+                 enum_blocks=None, scan_blocks=None, heavy_blocks=None, unit_rows=None,
+                 scan_claim=None, refute=True, verify=False):
         L = _lib()
+        if L.pac_abi_version() != 2:
+            raise RuntimeError("libpac.so ABI %d, this binding expects 2" % L.pac_abi_version())
         o = Options()
         L.pac_default_options(ctypes.byref(o))
         o.device = device
@@ -184,10 +190,12 @@ class Engine:
         if queue_entries:
             o.reserved_u[0] = int(queue_entries)  # alpha-tetrahedron queue size (testing)
         o.autotune = int(bool(autotune))
-        if handoff:
-            o.reserved_i[0] = int(handoff)  # launch-shape overrides
-        if scan_blocks:
-            o.reserved_i[1] = int(scan_blocks)
+        # launch-shape overrides (include/pac.h, pac_options.reserved_i)
+        for k, v in enumerate((enum_blocks, scan_blocks, heavy_blocks, unit_rows, scan_claim)):
+            if v:
+                o.reserved_i[k] = int(v)
+        o.reserved_i[5] = 0 if refute else 1
+        o.reserved_i[6] = 1 if verify else 0
         self._ctx = ctypes.c_void_p()
         _check(L.pac_create(ctypes.byref(self._ctx), ctypes.byref(o)))
 

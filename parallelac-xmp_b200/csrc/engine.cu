@@ -77,6 +77,20 @@ void Arena::reset() {
     cur_ = 0;
 }
 
+Arena::Mark Arena::mark() const {
+    if (cur_ >= blocks_.size()) return Mark{cur_, 0};
+    return Mark{cur_, blocks_[cur_].used};
+}
+
+void Arena::rewind(const Mark &m) {
+    // blocks past the mark's were empty when it was taken (alloc only moves
+    // forward and fresh or reset blocks start empty); blocks added since
+    // stay reserved for the next call
+    for (size_t k = m.block + 1; k < blocks_.size(); k++) blocks_[k].used = 0;
+    if (m.block < blocks_.size()) blocks_[m.block].used = m.used;
+    cur_ = std::min(m.block, blocks_.size());
+}
+
 size_t Arena::reserved() const {
     size_t t = 0;
     for (auto &b : blocks_) t += b.size;
@@ -95,15 +109,17 @@ __global__ void k_check_finite(const float4 *b, uint64_t n, int *bad) {
     if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) *bad = 1;
 }
 
-// Launch shapes for the autotuner (pac_options.autotune): the cooperative
-// hand-off threshold of the orthosphere scan (kNoHandoff: a lane finishes
-// every tetrahedron it takes) and its blocks per SM.  The first is the
-// default: on the 100k-ball globule the hand-off cost more than it saved
-// (30.1 ms without it, 31.2 at 32 balls, 34.3 at 8).
-constexpr int kNoHandoff = 1 << 30;
-constexpr pac::LaunchShape kShapes[] = {{kNoHandoff, 4}, {kNoHandoff, 3}, {kNoHandoff, 6},
-                                        {kNoHandoff, 2}, {256, 4}, {128, 4}, {64, 4}, {32, 4}};
+// Launch shapes for the autotuner (pac_options.autotune): blocks per SM of
+// the two tetrahedron enumeration kernels and of the orthosphere scan, the
+// rows of a large ball per enumeration work unit, and the queue entries a
+// scan warp claims at a time.  The first is the default.  None of them
+// changes the output.
+constexpr pac::LaunchShape kShapes[] = {
+    {4, 4, 4, 8, 512},  {3, 4, 4, 8, 512}, {2, 4, 4, 8, 512},  {4, 3, 4, 8, 512},
+    {4, 4, 3, 8, 512},  {4, 4, 6, 8, 512}, {4, 4, 4, 4, 512},  {4, 4, 4, 16, 512},
+    {4, 4, 4, 8, 128},  {4, 4, 4, 8, 2048}, {2, 2, 2, 8, 512}, {4, 2, 4, 4, 512}};
 constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+static_assert(kNumShapes <= 16, "Tuner holds 16 timings");
 
 int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
         const uint64_t *h_off, float sol, float alpha, pac::PassOutput &out, pac_stats *st) {
@@ -121,8 +137,8 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
         return pac::set_error(PAC_ERR_CUDA, std::string("input check: ") + cudaGetErrorString(e));
     if (hbad) return pac::set_error(PAC_ERR_INVALID_ARG, "non-finite ball coordinate or radius");
     // the alpha-tetrahedron queue: a quarter of the free memory at the
-    // context's first pass, at most 12 GiB (32 B per entry); a pass larger
-    // than that runs in chunks
+    // context's first pass, at most 12 GiB (32 B per entry); a pass whose
+    // queued tetrahedra exceed it runs in chunks
     if (!c.queue_bytes) {
         size_t freeb = 0, totalb = 0;
         cudaMemGetInfo(&freeb, &totalb);
@@ -130,19 +146,29 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
     }
     uint64_t qbytes = c.queue_bytes;
     if (c.opt.reserved_u[0]) qbytes = c.opt.reserved_u[0] * 32ull;  // test hook: entries
-    pac::PipelineConfig cfg{c.opt.formula, c.opt.tet_mode, c.opt.verbose, qbytes / 32,
-                            c.opt.predicates == PAC_PRED_EXACT, kShapes[0].handoff,
-                            kShapes[0].scan_blocks};
+    const pac::LaunchShape *shape = &kShapes[0];
     // launch shapes: the caller's overrides, else the autotuner's current
     // candidate or its choice, else the defaults
+    bool overridden = false;
+    for (int k = 0; k < 5; k++) overridden |= c.opt.reserved_i[k] > 0;
     int cand = -1;
-    if (c.opt.autotune && !c.opt.reserved_i[0] && !c.opt.reserved_i[1]) {
+    if (c.opt.autotune && !overridden) {
         cand = c.tuner.best >= 0 ? c.tuner.best : c.tuner.next;
-        cfg.handoff = kShapes[cand].handoff;
-        cfg.scan_blocks = kShapes[cand].scan_blocks;
+        shape = &kShapes[cand];
     }
-    if (c.opt.reserved_i[0] > 0) cfg.handoff = c.opt.reserved_i[0];
-    if (c.opt.reserved_i[1] > 0) cfg.scan_blocks = c.opt.reserved_i[1];
+    pac::PipelineConfig cfg{};
+    cfg.formula = c.opt.formula;
+    cfg.tet_mode = c.opt.tet_mode;
+    cfg.verbose = c.opt.verbose;
+    cfg.queue_entries = qbytes / 32;
+    cfg.exact = c.opt.predicates == PAC_PRED_EXACT;
+    cfg.refute = c.opt.reserved_i[5] != 1;
+    cfg.verify = c.opt.reserved_i[6] == 1;
+    cfg.enum_blocks = c.opt.reserved_i[0] > 0 ? c.opt.reserved_i[0] : shape->enum_blocks;
+    cfg.scan_blocks = c.opt.reserved_i[1] > 0 ? c.opt.reserved_i[1] : shape->scan_blocks;
+    cfg.heavy_blocks = c.opt.reserved_i[2] > 0 ? c.opt.reserved_i[2] : shape->heavy_blocks;
+    cfg.unit_rows = c.opt.reserved_i[3] > 0 ? c.opt.reserved_i[3] : shape->unit_rows;
+    cfg.scan_claim = c.opt.reserved_i[4] > 0 ? c.opt.reserved_i[4] : shape->scan_claim;
     pac_stats local;
     pac_stats *sp = st ? st : &local;
     pac::PassInput in{d_balls, n, n_mol, h_off, sol, alpha};
@@ -496,9 +522,15 @@ int pac_union_measure(pac_ctx *ctx, const double *xyzr, uint32_t n, const pac_co
     if (!ctx || !cx || (n && !xyzr)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
     if (cx->n_vertices && cx->n_vertices != n)
         return pac::set_error(PAC_ERR_INVALID_ARG, "complex and balls differ in size");
+    if (cx->on_device == 1 &&
+        ((cx->n_edges && !cx->edges) || (cx->n_tris && !cx->tris) || (cx->n_tets && !cx->tets)))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "a non-empty list has a null pointer");
     pac::Ctx &c = ctx->c;
     cudaSetDevice(c.device);
-    // no arena reset: a device complex from the previous call may live there
+    // no arena reset: a device complex from the previous call may live
+    // there; this call's copies and scratch go back to the pool on return,
+    // so repeated calls do not grow it
+    pac::ArenaRewind rewind(c.arena);
     double4 *d = c.arena.alloc_n<double4>(n);
     if (!d) return PAC_ERR_OOM;
     cudaMemcpyAsync(d, xyzr, sizeof(double4) * n, cudaMemcpyHostToDevice, c.stream);
@@ -541,8 +573,15 @@ int pac_union_measure_device(pac_ctx *ctx, const double *d_xyzr, uint32_t n, con
     if (!ctx || !cx || (n && !d_xyzr)) return pac::set_error(PAC_ERR_INVALID_ARG, "null argument");
     if (cx->on_device != 1)
         return pac::set_error(PAC_ERR_INVALID_ARG, "pac_union_measure_device needs device lists");
+    if (cx->n_vertices && cx->n_vertices != n)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "complex and balls differ in size");
+    if ((cx->n_edges && !cx->edges) || (cx->n_tris && !cx->tris) || (cx->n_tets && !cx->tets))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "a non-empty list has a null pointer");
     pac::Ctx &c = ctx->c;
     cudaSetDevice(c.device);
+    // scratch of this call (partial sums, gradients not passed) is handed
+    // back to the pool on return: repeated calls do not grow it
+    pac::ArenaRewind rewind(c.arena);
     return pac::union_measure_device(c, reinterpret_cast<const double4 *>(d_xyzr), n, cx->edges,
                                      cx->n_edges, cx->tris, cx->n_tris, cx->tets, cx->n_tets, vol,
                                      area, d_dvol, d_darea, nullptr);

@@ -26,6 +26,15 @@ class Arena {
     }
     void reset();
     size_t reserved() const;
+    // A position in the pool: rewind() releases everything allocated after
+    // mark() was taken, keeping what came before (e.g. a complex that the
+    // caller still holds).  The memory released must no longer be in use by
+    // queued work other than on the context's own stream.
+    struct Mark {
+        size_t block, used;
+    };
+    Mark mark() const;
+    void rewind(const Mark &m);
 
    private:
     struct Block {
@@ -36,20 +45,35 @@ class Arena {
     size_t cur_ = 0;
 };
 
+// Rewinds the pool to where it was at construction, on every return path.
+struct ArenaRewind {
+    Arena &a;
+    Arena::Mark m;
+    explicit ArenaRewind(Arena &arena) : a(arena), m(arena.mark()) {}
+    ~ArenaRewind() { a.rewind(m); }
+    ArenaRewind(const ArenaRewind &) = delete;
+    ArenaRewind &operator=(const ArenaRewind &) = delete;
+};
+
 struct PipelineConfig {
     int formula;    // pac_formula
     int tet_mode;   // pac_tet_mode
     int verbose;
     uint64_t queue_entries;  // alpha tetrahedra queued per chunk (32 B each)
     bool exact;              // decision-exact predicates (strict flavour only)
+    bool refute;             // early refutation in the tetrahedron enumeration
+    bool verify;             // replay every certified insphere decision (debug)
     // launch shapes (the output does not depend on them)
-    int handoff;      // window balls a scan lane tests alone before the warp takes over
-    int scan_blocks;  // k_tets_scan blocks per SM
+    int enum_blocks;   // k_tets_enum<.., 1> blocks per SM
+    int heavy_blocks;  // k_tets_enum<.., kMaxW> blocks per SM
+    int scan_blocks;   // k_tets_scan blocks per SM
+    int unit_rows;     // rows of a ball of more than 64 upper neighbours per work unit
+    int scan_claim;    // queue entries a scan warp claims at a time
 };
 
 // Launch shapes the autotuner tries, and its state per context.
 struct LaunchShape {
-    int handoff, scan_blocks;
+    int enum_blocks, heavy_blocks, scan_blocks, unit_rows, scan_claim;
 };
 struct Tuner {
     int next = 0;          // next candidate to measure

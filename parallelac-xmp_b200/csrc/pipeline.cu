@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "certify.cuh"
 #include "exactpred.cuh"
 #include "pac_internal.h"
 #include "refarith.cuh"
@@ -49,12 +50,14 @@ constexpr unsigned kFull = 0xffffffffu;
 enum Counter {
     C_CAND_E, C_ALPHA_E, C_CAND_T, C_ALPHA_T, C_CAND_Q, C_ALPHA_Q, C_INSPHERE, C_SOS,
     C_OOB, C_SURV, C_PEND, C_MAXDEG, C_SOS_RANGE, C_BADDEG, C_NEXT, C_FILTER, C_FALLBACK,
+    C_KILLED, C_KTESTS, C_CERT, C_CERT_BAD,
     C_NCOUNTERS
 };
 
 struct MolGrid {
     float minx, miny, minz, step;
-    int gx, gy, gz, pad;
+    int gx, gy, gz;
+    float wmax;  // upper bound on every ball's binary32 weight (r + sol)^2
     uint64_t cell_base;  // first global cell of this molecule
     uint64_t ncell;
     uint64_t atom_base;  // first ball (sorted and input) of this molecule
@@ -395,7 +398,8 @@ __global__ void k_bbox(const float4 *balls, uint64_t n, const uint32_t *mol, int
 }
 
 // grid parameters per molecule (AlphaComplexLargeData.cu:1119-1123)
-__global__ void k_grid(const int *mm, uint32_t n_mol, float alpha, MolGrid *g, uint64_t *ncell) {
+__global__ void k_grid(const int *mm, uint32_t n_mol, float sol, float alpha, MolGrid *g,
+                       uint64_t *ncell) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n_mol) return;
     float minX = funkey(mm[m * 8 + 0]), minY = funkey(mm[m * 8 + 1]),
@@ -415,7 +419,11 @@ __global__ void k_grid(const int *mm, uint32_t n_mol, float alpha, MolGrid *g, u
     r.gx = gx;
     r.gy = gy;
     r.gz = gz;
-    r.pad = 0;
+    // r + sol is rounded monotonically, so the extreme radii bound every
+    // ball's weight; the margin covers the rounding of the square
+    const float rlo = fabsf(__fadd_rn(funkey(mm[m * 8 + 3]), sol)), rhi = fabsf(__fadd_rn(maxRadius, sol));
+    const float rm = fmaxf(rlo, rhi);
+    r.wmax = __fmul_rn(__fmul_rn(rm, rm), 1.0f + 1.0f / 1024.0f);
     r.cell_base = 0;
     r.ncell = (uint64_t)max(gx, 0) * (uint64_t)max(gy, 0) * (uint64_t)max(gz, 0);
     r.atom_base = 0;
@@ -698,9 +706,12 @@ struct TetArgs {
     uint64_t pend_cap;
     const uint64_t *toff; // as-run fill: output offsets per ball
     uint32_t *tets_out;   // as-run fill: sorted-space vertex quadruples
-    unsigned long long *ctr;
-    unsigned long long *gctr;  // the pass's counters (ctr may be a chunk's)
-    int handoff;               // scan: window balls a lane tests alone
+    unsigned long long *ctr;   // the pass's counters, or a chunk's (enumeration)
+    const uint32_t *cellof;    // global cell of each sorted ball
+    int refute;                // enumeration: refute early against the group's best candidate
+    int verify;                // scan: replay every certified decision and count disagreements
+    int unit_rows;             // rows of a large ball per enumeration work unit
+    int scan_claim;            // queue entries a scan warp claims at a time
 };
 
 __device__ __forceinline__ void mark_face(uint64_t *F, uint64_t row_base, int W, int a, int b) {
@@ -848,26 +859,38 @@ __device__ __forceinline__ uint32_t key_of(const uint32_t *N, int deg, uint32_t 
            ((uint32_t)lbound(N, deg, v4) << 16);
 }
 
-__device__ __noinline__ void emit_survivor(const TetArgs &A, uint64_t p, int W, uint64_t lp,
-                                              const uint32_t *N, uint32_t key, bool pending,
-                                              uint32_t &ball_count) {
+// Records one tetrahedron that passed the orthosphere test (or, pending,
+// one whose window held an exact zero): the survivor list, the per-ball
+// count, and the marks of its four faces in the `faces` matrices.
+__device__ __noinline__ void emit_survivor(const uint64_t *__restrict__ eoff,
+                                           const uint32_t *__restrict__ ER,
+                                           const uint64_t *__restrict__ loff, uint64_t *faces,
+                                           uint2 *surv, uint64_t surv_cap, uint2 *pend,
+                                           uint64_t pend_cap, unsigned long long *ctr,
+                                           uint32_t *tcount, uint32_t p, uint32_t v2, uint32_t v3,
+                                           uint32_t v4, bool pending) {
+    const uint64_t e0 = eoff[p];
+    const int deg = (int)(eoff[p + 1] - e0);
+    const uint32_t *N = ER + e0;
+    const uint32_t key = key_of(N, deg, v2, v3, v4);
     if (pending) {
-        unsigned long long q = atomicAdd(&A.ctr[C_PEND], 1ull);
-        if (q < A.pend_cap) A.pend[q] = make_uint2((uint32_t)p, key);
+        unsigned long long q = atomicAdd(&ctr[C_PEND], 1ull);
+        if (q < pend_cap) pend[q] = make_uint2(p, key);
         return;
     }
-    unsigned long long q = atomicAdd(&A.ctr[C_SURV], 1ull);
-    if (q < A.surv_cap) A.surv[q] = make_uint2((uint32_t)p, key);
-    ball_count++;
-    int a = key & 0xff, b = (key >> 8) & 0xff, c = (key >> 16) & 0xff;
-    mark_face(A.faces, lp, W, a, b);
-    mark_face(A.faces, lp, W, a, c);
-    mark_face(A.faces, lp, W, b, c);
-    const uint32_t v2 = N[a];
-    const uint64_t e2 = A.eoff[v2];
-    const int deg2 = (int)(A.eoff[v2 + 1] - e2);
-    const int mb = lbound(A.ER + e2, deg2, N[b]), mc = lbound(A.ER + e2, deg2, N[c]);
-    mark_face(A.faces, A.loff[v2], (deg2 + 63) >> 6, mb, mc);
+    unsigned long long q = atomicAdd(&ctr[C_SURV], 1ull);
+    if (q < surv_cap) surv[q] = make_uint2(p, key);
+    atomicAdd(&tcount[p], 1u);
+    const int W = (deg + 63) >> 6;
+    const uint64_t lp = loff[p];
+    const int a = key & 0xff, b = (key >> 8) & 0xff, c = (key >> 16) & 0xff;
+    mark_face(faces, lp, W, a, b);
+    mark_face(faces, lp, W, a, c);
+    mark_face(faces, lp, W, b, c);
+    const uint64_t e2 = eoff[v2];
+    const int deg2 = (int)(eoff[v2 + 1] - e2);
+    const int mb = lbound(ER + e2, deg2, v3), mc = lbound(ER + e2, deg2, v4);
+    mark_face(faces, loff[v2], (deg2 + 63) >> 6, mb, mc);
 }
 
 // The 27-cell window of the orthosphere and attachment tests, visited as
@@ -929,104 +952,172 @@ __device__ __forceinline__ void window_centre(const MolGrid &G, const uint32_t *
     end = cellbeg[G.cell_base + (uint64_t)cl.w + 1];
 }
 
-constexpr int kLongCap = 64;   // tetrahedra handed to the cooperative scan
-// Queue entries a warp of k_tets_scan claims at a time: one counter serves
-// every warp, and claims of 32 made the atomics a bottleneck (25.6 ms for
-// the stage at 100k balls; 24.4 with 128, 24.2 with 512).
-constexpr uint64_t kScanClaim = 512;
-
-// Cooperative empty-orthosphere test of one tetrahedron by the whole warp:
-// lane 0 owns the centre cell, lanes 1..10 the window's other parts, and a
-// prefix sum over their sizes flattens the window balls over the lanes.  Returns 1 = violated,
-// 2 = no violation but an exact zero, 0 = empty.
-template <int V>
-__device__ __noinline__ int coop_test(const TetArgs &A, const MolGrid &G, uint32_t v1,
-                                         uint32_t v2, uint32_t v3, uint32_t v4, const float *pa,
-                                         const float *pb, const float *pc, const float *pd,
-                                         float wa, float wb, float wc, float wd,
-                                         float orientation, int4 cl,
-                                         unsigned long long &evals, Tally &tally) {
-    const int lane = threadIdx.x & 31;
-    uint32_t beg = 0, cnt = 0;
-    if (lane == 0) {  // the centre cell
-        unsigned long long none = 0;
-        uint32_t end = 0;
-        window_centre(G, A.cellbeg, cl, beg, end, none);
-        cnt = end - beg;
-    } else if (lane <= kWindowParts) {
-        uint32_t end = 0;
-        if (window_part(G, A.cellbeg, cl.x, cl.y, cl.z, lane - 1, beg, end)) cnt = end - beg;
-    }
-    uint32_t incl = cnt;
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t v = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    bool zero = false;
-    for (uint32_t base = 0; base < total; base += 32) {
-        uint32_t s = base + lane;
-        int lo = 0;
-        for (int step = 16; step; step >>= 1) {
-            uint32_t v = __shfl_sync(kFull, incl, lo + step - 1);
-            if (v <= s) lo += step;
-        }
-        const uint32_t sinc = __shfl_sync(kFull, incl, lo & 31);
-        const uint32_t sbeg = __shfl_sync(kFull, beg, lo & 31);
-        const uint32_t scnt = __shfl_sync(kFull, cnt, lo & 31);
-        bool viol = false;
-        if (s < total) {
-            uint32_t x = sbeg + (s - (sinc - scnt));
-            if (!(x == v1 || x == v2 || x == v3 || x == v4)) {
-                const Ball atom = pac::ld_ball(&A.at[x]);
-                float pe[3];
-                pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-                float we = wt<V>(atom.r);
-                evals++;
-                float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
-                viol = orientation < 0 ? (result < 0) : (result > 0);
-                if (result == 0) zero = true;
-            }
-        }
-        if (__any_sync(kFull, viol)) return 1;
-    }
-    return __any_sync(kFull, zero) ? 2 : 0;
+// Cell coordinate (int)((p - lo) / step) of the reference (LD:621-623), with
+// the IEEE division replaced by a multiplication by inv = fl(1 / step)
+// whenever that provably truncates to the same integer: the product is
+// within 3.1 ulp of the quotient, so when no integer lies within 16 ulp of
+// it both truncate alike.  Otherwise (and for huge or non-finite values)
+// the division itself.
+__device__ __forceinline__ int cell_coord_fast(float p, float lo, float step, float inv) {
+    const float d = __fsub_rn(p, lo);
+    const float q = __fmul_rn(d, inv);
+    const float t = truncf(q);
+    const float f = fabsf(__fsub_rn(q, t));
+    if (fabsf(q) < 4194304.0f && fminf(f, __fsub_rn(1.0f, f)) > 16.0f * pac::cert::kU * fabsf(q) + 1e-30f)
+        return (int)t;
+    return pac::cell_coord(p, lo, step);
 }
 
+// The window cell of an orthosphere centre: (gridX, gridY, gridZ, wrapped
+// linear index), as the reference forms it (LD:621-626).
+__device__ __forceinline__ int4 window_cell(const MolGrid &G, float x, float y, float z) {
+    const float inv = __frcp_rn(G.step);
+    const int gX = cell_coord_fast(x, G.minx, G.step, inv);
+    const int gY = cell_coord_fast(y, G.miny, G.step, inv);
+    const int gZ = cell_coord_fast(z, G.minz, G.step, inv);
+    return make_int4(gX, gY, gZ, lin3(gX, gY, gZ, G.gx, G.gy));
+}
+
+// Whether the reference's window of an orthosphere centre (x, y, z) holds
+// a ball at (bx, by, bz) in the grid: certainly so when the two are less
+// than 0.99 cell steps apart on every axis.  The cells are truncations of
+// the monotone binary32 map v -> (v - lo) / step (LD:72-74, 621-623), so the
+// two quotients differ by less than one (the rounding is far below the 1 %
+// margin for grids of at most 16384 cells per axis); the ball's quotient is
+// non-negative, so the centre's truncated cell is never below -0 and the
+// ball's cell lies within one of it per axis.  A centre cell inside the grid
+// is read as itself; outside the grid the ball's cell differs from it and is
+// one of the 26 in-grid neighbours.  Either way the reference visits it.
+__device__ __forceinline__ bool surely_in_window(float x, float y, float z, float bx, float by,
+                                                 float bz, float reach) {
+    return fmaxf(fabsf(bx - x), fmaxf(fabsf(by - y), fabsf(bz - z))) <= reach;
+}
+
+// Queue slots are handed out to warps in blocks (one atomic per block, not
+// per batch: a single counter served every warp).  Slots a warp reserved
+// but did not fill are marked with this ball index, and the scan skips them.
+constexpr uint32_t kNoTet = 0xffffffffu;
+constexpr uint64_t kQBlock = 128;
+
 // ---- the as-written tetrahedra: enumeration, then a scan over an HBM queue
-// Enumeration (k_tets_alpha1, k_tets_alpha_rows, through tet_row): the
-// candidate fourth vertices of every alpha triangle (v1, v2, v3) are
-// flattened over the lanes (common bits of rows a and b of v1's link matrix,
-// checked against v2's link matrix: the reference's candidate tetrahedra,
-// AlphaComplexLargeData.cu:350-529), each lane applies markRealTets to one
-// candidate, and the passing tetrahedra are appended to the queue with the
-// cell of their orthosphere centre.
+// Enumeration (k_tets_enum): ball p's candidate tetrahedra are the
+// (p, v2 = N[a], v3 = N[b], v4 = N[c]), a < b < c, with (p, v2, v3),
+// (p, v2, v4), (p, v3, v4) alpha triangles (bits of p's link rows) and
+// (v2, v3, v4) one too (a bit of v2's link matrix) -- exactly the
+// reference's candidates (AlphaComplexLargeData.cu:350-529).  Per row a the
+// candidate set of every triangle group (a, b) is built bitwise, the pairs
+// (b, c) are written group by group to a per-warp list in shared memory, and
+// the list is evaluated 32 at a time with every lane busy: markRealTets,
+// then an early refutation, then the queue.
+//
+// Early refutation.  Within one group the fourth vertices lie in the pencil
+// of spheres orthogonal to the balls p, v2, v3; on either side of the
+// triangle's plane the candidate whose orthosphere comes first along the
+// pencil lies inside the orthosphere of every other candidate on that side.
+// Each lane's tetrahedron is therefore tested against the best candidate
+// of its group and side found so far (a shared-memory minimum over the
+// lanes' orthocentres projected on the triangle normal), with the
+// reference's own arithmetic (orient3d, insphere_w), provided that ball lies
+// in the reference's window of the tetrahedron (surely_in_window).  A violation there is a
+// violation the reference finds: the tetrahedron is dropped.  The rest
+// (a few per cent) go to the queue.
 struct TetQueue {
-    uint4 *vid;       // (v1, v2, v3, v4): the scan loads the balls directly
-    int4 *cell;       // (gridX, gridY, gridZ, linear centre index)
+    uint4 *vid;    // (v1, v2, v3, v4); v1 = kNoTet marks an unused slot
+    float4 *sph;   // orthosphere centre (x, y, z) and power of v2, as markRealTets gives them
     uint64_t cap;
 };
 
-// One row a of ball v1's candidate tetrahedra (v1, v2 = N[a], v3, v4).  The
-// caller has staged v1's upper neighbours in N and their balls in sb (both
-// in shared memory, indexed by position, at least from a on); L holds v1's
-// link rows (W words each, shared or global memory).  v2's neighbour list and link rows are staged here, in
-// sN2 and sL2 (when they fit: at most L2CAP words), so the candidate loop
-// reads no global memory but the queue it appends to.
-template <int V, int KW, int L2CAP>
-__device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uint64_t p, int a,
-                                        int deg, int W, const uint32_t *N, const uint64_t *L,
-                                        const float4 *sb, uint32_t *sN2, uint64_t *sL2,
-                                        uint16_t *smap, const Ball B1, const MolGrid &G,
-                                        unsigned long long &cand_acc,
-                                        unsigned long long &alpha_acc, Tally &tally) {
+template <int KW>
+struct EnumSmem;
+// balls of at most 64 upper neighbours: one link word per row, all staged
+template <>
+struct EnumSmem<1> {
+    static constexpr int kDeg = 64, kL2Cap = 64, kCandCap = 256, kWarps = 8;
+    float4 sb[kWarps][kDeg];      // balls of p's upper neighbours
+    uint64_t sL[kWarps][kDeg];    // p's link rows
+    uint64_t sL2[kWarps][kL2Cap]; // v2's link rows (when they fit)
+    uint32_t sN2[kWarps][kMaxDeg];// v2's upper neighbours
+    uint32_t sN[kWarps][kDeg];    // p's upper neighbours
+    uint16_t smap[kWarps][kDeg];  // position of N[c] in v2's list, 0xffff: absent
+    uint16_t cand[kWarps][kCandCap];  // (b-chunk index j) | c << 8
+    uint8_t sBl[kWarps][kDeg];    // the b's of the row, ascending
+    unsigned long long best[kWarps][64];  // per (j, side): orderable key << 32 | c
+};
+// larger balls: rows read in place, v2's rows staged when they fit
+template <>
+struct EnumSmem<kMaxW> {
+    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kCandCap = 512, kWarps = 4;
+    float4 sb[kWarps][kDeg];
+    uint64_t sL2[kWarps][kL2Cap];
+    uint32_t sN2[kWarps][kMaxDeg];
+    uint32_t sN[kWarps][kDeg];
+    uint16_t smap[kWarps][kDeg];
+    uint16_t cand[kWarps][kCandCap];
+    uint8_t sBl[kWarps][kDeg];
+    unsigned long long best[kWarps][64];
+};
+
+// Per-warp state of the queue reservation.
+struct QRes {
+    uint64_t pos, end;  // next free slot of the warp's block, its end
+};
+
+// Appends the lanes with `take` to the queue (warp-uniform call).
+__device__ __forceinline__ void queue_append(const TetQueue &Q, unsigned long long *ctr, QRes &qr,
+                                             bool take, uint4 vid, float4 sph) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(kFull, take);
+    if (!m) return;
+    const int k = __popc(m), rank = __popc(m & ((1u << lane) - 1));
+    const uint64_t left = qr.end - qr.pos;
+    uint64_t nb = 0;
+    if ((uint64_t)k > left) {
+        if (lane == 0) nb = atomicAdd(&ctr[C_SURV], (unsigned long long)kQBlock);
+        nb = __shfl_sync(kFull, nb, 0);
+    }
+    if (take) {
+        const uint64_t pos = (uint64_t)rank < left ? qr.pos + rank : nb + (rank - left);
+        if (pos < Q.cap) {
+            Q.vid[pos] = vid;
+            Q.sph[pos] = sph;
+        }
+    }
+    if ((uint64_t)k > left) {
+        qr.pos = nb + (k - left);
+        qr.end = nb + kQBlock;
+    } else {
+        qr.pos += k;
+    }
+}
+
+// Marks the rest of the warp's block unused.
+__device__ __forceinline__ void queue_close(const TetQueue &Q, QRes &qr) {
+    const int lane = threadIdx.x & 31;
+    for (uint64_t s = qr.pos + lane; s < qr.end; s += 32)
+        if (s < Q.cap) Q.vid[s] = make_uint4(kNoTet, 0, 0, 0);
+    qr.pos = qr.end;
+}
+
+// One row a of ball p: v2 = N[a].  N, sb, sCell hold p's upper neighbours,
+// their balls and cells (shared memory); L its link rows (W words each,
+// shared or global); the rest is per-warp scratch.
+template <int V, int KW>
+__device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, EnumSmem<KW> &S,
+                                        const int wib, QRes &qr, uint32_t p, int a, int deg, int W,
+                                        const uint64_t *L, const Ball B1, const MolGrid &G,
+                                        bool refute, unsigned long long &cand_acc,
+                                        unsigned long long &alpha_acc, unsigned long long &kill_acc,
+                                        unsigned long long &ktest_acc, Tally &tally) {
+    constexpr int kL2Cap = EnumSmem<KW>::kL2Cap, kCandCap = EnumSmem<KW>::kCandCap;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
+    const uint32_t *N = S.sN[wib];
+    const float4 *sb = S.sb[wib];
     uint64_t ra[KW];
     int nb = 0;
 #pragma unroll
     for (int w = 0; w < KW; w++) {
-        ra[w] = w < W ? L[(uint64_t)a * W + w] : 0;
+        ra[w] = w < W ? L[(uint64_t)a * W + w] : 0ull;
         nb += __popcll(ra[w]);
     }
     if (nb < 2) return;
@@ -1034,15 +1125,36 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
     const uint64_t e2 = A.eoff[v2];
     const int deg2 = (int)(A.eoff[v2 + 1] - e2);
     const int W2 = (deg2 + 63) >> 6;
-    const uint64_t *L2 = A.link + A.loff[v2];
-    const bool l2s = deg2 * W2 <= L2CAP;  // v2's rows staged
+    const uint64_t *L2g = A.link + A.loff[v2];
+    const bool l2s = deg2 * W2 <= kL2Cap;
+    uint32_t *sN2 = S.sN2[wib];
+    uint64_t *sL2 = S.sL2[wib];
+    uint16_t *smap = S.smap[wib];
+    uint8_t *sBl = S.sBl[wib];
     for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
     if (l2s)
-        for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2[k];
+        for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2g[k];
+    // the b's of the row, ascending
+#pragma unroll
+    for (int w = 0; w < KW; w++) {
+        if (w >= W) break;
+        int before = 0;
+#pragma unroll
+        for (int v = 0; v < KW; v++)
+            if (v < w) before += __popcll(ra[v]);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const bool bit = (ra[w] >> (32 * h + lane)) & 1ull;
+            const unsigned bm = __ballot_sync(kFull, bit);
+            const int lo = (int)__popcll(ra[w] & ((1ull << (32 * h)) - 1ull)) * (h ? 1 : 0);
+            if (bit) sBl[before + lo + __popc(bm & lt_mask)] = (uint8_t)(w * 64 + 32 * h + lane);
+        }
+    }
     __syncwarp();
+    // position of N[c] in v2's list, for c > a
     for (int c = a + 1 + lane; c < deg; c += 32) {
         const uint32_t x = N[c];
-        int lo2 = 0, n2 = deg2;  // lower bound of x in v2's list
+        int lo2 = 0, n2 = deg2;
         while (n2 > 0) {
             const int h = n2 >> 1;
             if (sN2[lo2 + h] < x) {
@@ -1055,400 +1167,385 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, uin
         smap[c] = (lo2 < deg2 && sN2[lo2] == x) ? (uint16_t)lo2 : (uint16_t)0xffff;
     }
     __syncwarp();
+    const float e12x = sb[a].x - B1.x, e12y = sb[a].y - B1.y, e12z = sb[a].z - B1.z;
     const float4 b2 = sb[a];
     const Ball B2{b2.x, b2.y, b2.z, b2.w};
+    // groups (a, b) in chunks of 32 b's, lane j owning group j
     for (int k0 = 0; k0 < nb; k0 += 32) {
-        const int b = (k0 + lane < nb) ? select_bit(ra, W, k0 + lane) : -1;
-        uint64_t m[KW];
+        const int nj = min(32, nb - k0);
+        // lane j: the fourth vertices c > b with the three faces at p
+        // (ra & L[b] & above b) whose face (v2, v3, v4) is in v2's link
+        uint64_t pm[KW];
+        int mb = 0xffff;
+        const uint64_t *R2 = sL2;
+        if (lane < nj) {
+            const int b = sBl[k0 + lane];
+            mb = smap[b];
+            R2 = l2s ? sL2 + mb * W2 : L2g + (uint64_t)mb * W2;
+#pragma unroll
+            for (int w = 0; w < KW; w++)
+                pm[w] = (w < W && mb != 0xffff) ? (ra[w] & L[(uint64_t)b * W + w] & above_mask(b, w))
+                                                : 0ull;
+        } else {
+#pragma unroll
+            for (int w = 0; w < KW; w++) pm[w] = 0ull;
+        }
+        // count pass (face check per bit), then write pass below
         int cnt = 0;
 #pragma unroll
         for (int w = 0; w < KW; w++) {
-            m[w] = (b >= 0 && w < W) ? (ra[w] & L[(uint64_t)b * W + w] & above_mask(b, w)) : 0;
-            cnt += __popcll(m[w]);
+            uint64_t bits = pm[w];
+            while (bits) {
+                const int c = w * 64 + __ffsll((long long)bits) - 1;
+                bits &= bits - 1;
+                const int mc = smap[c];
+                if (mc != 0xffff && ((R2[mc >> 6] >> (mc & 63)) & 1ull)) cnt++;
+                else pm[w] &= ~(1ull << (c & 63));
+            }
         }
         int incl = cnt;
         for (int o = 1; o < 32; o <<= 1) {
-            int v = __shfl_up_sync(kFull, incl, o);
+            const int v = __shfl_up_sync(kFull, incl, o);
             if (lane >= o) incl += v;
         }
         const int total = __shfl_sync(kFull, incl, 31);
-        for (int base = 0; base < total; base += 32) {
-            const int s = base + lane;
-            int lo3 = 0;
-            for (int step = 16; step; step >>= 1) {
-                int v = __shfl_sync(kFull, incl, lo3 + step - 1);
-                if (v <= s) lo3 += step;
-            }
-            const int owner = lo3 & 31;
-            const int oincl = __shfl_sync(kFull, incl, owner);
-            const int ocnt = __shfl_sync(kFull, cnt, owner);
-            const int bo = __shfl_sync(kFull, b, owner);
-            uint64_t mo[KW];
+        if (lane == 0) cand_acc += total;
+        // best-so-far slots of the chunk's groups (j, side)
+        S.best[wib][lane] = ~0ull;
+        S.best[wib][lane + 32] = ~0ull;
+        const int myoff = incl - cnt;
+        // the chunk's candidates, group by group, kCandCap at a time
+        for (int base = 0; base < total; base += kCandCap) {
+            __syncwarp();
+            {
+                int idx = myoff;
 #pragma unroll
-            for (int w = 0; w < KW; w++) {
-                uint32_t l32 = __shfl_sync(kFull, (uint32_t)m[w], owner);
-                uint32_t h32 = __shfl_sync(kFull, (uint32_t)(m[w] >> 32), owner);
-                mo[w] = ((uint64_t)h32 << 32) | l32;
-            }
-            bool pass4 = false, passA = false;
-            int c = -1;
-            int4 cell = make_int4(0, 0, 0, 0);
-            if (s < total) {
-                c = select_bit(mo, W, s - (oincl - ocnt));
-                const int mb = smap[bo], mc = smap[c];
-                if (mb != 0xffff && mc != 0xffff) {
-                    const uint64_t at2 = (uint64_t)mb * W2 + (mc >> 6);
-                    const uint64_t word = l2s ? sL2[at2] : __ldg(&L2[at2]);
-                    pass4 = (word >> (mc & 63)) & 1ull;
-                }
-                if (pass4) {
-                    const float4 b3 = sb[bo], b4 = sb[c];
-                    const Ball B3{b3.x, b3.y, b3.z, b3.w}, B4{b4.x, b4.y, b4.z, b4.w};
-                    float4 sphere;
-                    passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
-                    if (passA) {
-                        int gridX = pac::cell_coord(sphere.x, G.minx, G.step);
-                        int gridY = pac::cell_coord(sphere.y, G.miny, G.step);
-                        int gridZ = pac::cell_coord(sphere.z, G.minz, G.step);
-                        cell = make_int4(gridX, gridY, gridZ, lin3(gridX, gridY, gridZ, G.gx, G.gy));
+                for (int w = 0; w < KW; w++) {
+                    uint64_t bits = pm[w];
+                    while (bits) {
+                        const int c = w * 64 + __ffsll((long long)bits) - 1;
+                        bits &= bits - 1;
+                        if (idx >= base && idx < base + kCandCap)
+                            S.cand[wib][idx - base] = (uint16_t)(lane | (c << 8));
+                        idx++;
                     }
                 }
             }
-            const unsigned m4 = __ballot_sync(kFull, pass4);
-            const unsigned mA = __ballot_sync(kFull, passA);
-            unsigned long long qbase = 0;
-            if (lane == 0 && mA) qbase = atomicAdd(&A.ctr[C_SURV], (unsigned long long)__popc(mA));
-            qbase = __shfl_sync(kFull, qbase, 0);
-            if (passA) {
-                uint64_t pos = qbase + __popc(mA & lt_mask);
-                if (pos < Q.cap) {
-                    Q.vid[pos] = make_uint4((uint32_t)p, v2, N[bo], N[c]);
-                    Q.cell[pos] = cell;
+            __syncwarp();
+            const int nwin = min(kCandCap, total - base);
+            for (int s0 = 0; s0 < nwin; s0 += 32) {
+                const bool act = s0 + lane < nwin;
+                int j = 0, c = 0;
+                if (act) {
+                    const uint32_t e = S.cand[wib][s0 + lane];
+                    j = (int)(e & 0xff);
+                    c = (int)(e >> 8);
                 }
-            }
-            if (lane == 0) {
-                cand_acc += __popc(m4);
-                alpha_acc += __popc(mA);
+                const int b = act ? (int)sBl[k0 + j] : 0;
+                bool passA = false, side = false;
+                float4 sphere = make_float4(0.f, 0.f, 0.f, 0.f);
+                float key = 0.f;
+                Ball B3{0.f, 0.f, 0.f, 0.f}, B4{0.f, 0.f, 0.f, 0.f};
+                if (act) {
+                    const float4 b3 = sb[b], b4 = sb[c];
+                    B3 = Ball{b3.x, b3.y, b3.z, b3.w};
+                    B4 = Ball{b4.x, b4.y, b4.z, b4.w};
+                    passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
+                    if (passA) {
+                        // the triangle (p, v2, v3)'s normal; the side of v4
+                        // and the pencil position of the orthocentre
+                        const float e13x = B3.x - B1.x, e13y = B3.y - B1.y, e13z = B3.z - B1.z;
+                        const float nx = e12y * e13z - e12z * e13y;
+                        const float ny = e12z * e13x - e12x * e13z;
+                        const float nz = e12x * e13y - e12y * e13x;
+                        side = nx * (B4.x - B1.x) + ny * (B4.y - B1.y) + nz * (B4.z - B1.z) > 0.f;
+                        key = nx * sphere.x + ny * sphere.y + nz * sphere.z;
+                        if (!side) key = -key;
+                    }
+                }
+                const unsigned mA = __ballot_sync(kFull, passA);
+                if (lane == 0) alpha_acc += __popc(mA);
+                bool keep = passA;
+                if constexpr (V != pac::kExact) {
+                    // the flat tetrahedra (orthocentre 0, LD:577-580) and
+                    // non-finite keys take no part
+                    const bool cand_best = refute && passA && isfinite(key) &&
+                                           !(sphere.x == 0.f && sphere.y == 0.f && sphere.z == 0.f);
+                    const int slot = j + (side ? 32 : 0);
+                    if (cand_best) {
+                        const uint32_t kb = __float_as_uint(key);
+                        const uint32_t ok = (kb & 0x80000000u) ? ~kb : (kb | 0x80000000u);
+                        atomicMin(&S.best[wib][slot], ((unsigned long long)ok << 32) | (uint32_t)c);
+                    }
+                    __syncwarp();
+                    if (cand_best) {
+                        const int y = (int)(S.best[wib][slot] & 0xffffffffull);
+                        const float4 by = sb[y];
+                        if (y != c && surely_in_window(sphere.x, sphere.y, sphere.z, by.x, by.y, by.z,
+                                                       0.99f * G.step)) {
+                            float pa[3] = {B1.x, B1.y, B1.z}, pb[3] = {B2.x, B2.y, B2.z};
+                            float pc[3] = {B3.x, B3.y, B3.z}, pd[3] = {B4.x, B4.y, B4.z};
+                            float pe[3] = {by.x, by.y, by.z};
+                            const float wa = wt<V>(B1.r), wb = wt<V>(B2.r), wc = wt<V>(B3.r),
+                                        wd = wt<V>(B4.r);
+                            const float ori = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
+                            const float res = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd,
+                                                              wt<V>(by.w), tally);
+                            ktest_acc++;
+                            if (ori < 0 ? (res < 0) : (res > 0)) {
+                                keep = false;
+                                kill_acc++;
+                            }
+                        }
+                    }
+                }
+                queue_append(Q, A.ctr, qr, keep,
+                             make_uint4(p, v2, act ? N[b] : 0u, act ? N[c] : 0u), sphere);
             }
         }
+        __syncwarp();
     }
     __syncwarp();
 }
 
-// k_tets_alpha1: balls of at most 64 upper neighbours (one link word per
-// row; most balls), one warp per ball, balls handed out from a counter over
-// the chunk [lo, hi).  The balls of v1's neighbours and v1's link rows are
-// staged in shared memory once per ball.
-template <int V>
-__global__ void __launch_bounds__(256, 4) k_tets_alpha1(TetArgs A, TetQueue Q, uint64_t lo,
-                                                        uint64_t hi) {
-    __shared__ float4 sb[8][64];          // balls of v1's upper neighbours
-    __shared__ uint64_t sL[8][64];        // v1's link rows
-    __shared__ uint64_t sL2[8][64];       // v2's link rows (when they fit)
-    __shared__ uint32_t sN2[8][kMaxDeg];  // v2's upper neighbours
-    __shared__ uint16_t smap[8][64];      // position of N[c] in v2's list, 0xffff: absent
-    __shared__ uint32_t sN[8][64];        // v1's upper neighbours
+// k_tets_enum: one warp per ball (KW = 1: balls of at most 64 upper
+// neighbours, taken from a counter over the chunk [lo, hi)) or per group of
+// A.unit_rows rows of a larger ball (KW = kMaxW: units from the prefix uoff of
+// k_heavy_rows over [lo, hi)).  The ball's neighbours, their balls and cells
+// (and, for KW = 1, its link rows) are staged in shared memory.
+template <int V, int KW>
+__global__ void __launch_bounds__(EnumSmem<KW>::kWarps * 32, KW == 1 ? 3 : 4)
+    k_tets_enum(TetArgs A, TetQueue Q, uint64_t lo, uint64_t hi, const uint64_t *uoff) {
+    // more than the 48 KB of static shared memory: dynamic, opted in by
+    // enum_smem_optin()
+    extern __shared__ __align__(16) unsigned char enum_smem[];
+    EnumSmem<KW> &S = *reinterpret_cast<EnumSmem<KW> *>(enum_smem);
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    unsigned long long cand_acc = 0, alpha_acc = 0;
+    unsigned long long cand_acc = 0, alpha_acc = 0, kill_acc = 0, ktest_acc = 0;
     Tally tally;
-    while (true) {
-        uint64_t p = 0;
-        if (lane == 0) {
-            // stop handing out balls once the queue has overflowed: the chunk
-            // is rerun smaller
-            p = (*(volatile unsigned long long *)&A.ctr[C_SURV] > Q.cap)
-                    ? hi
-                    : lo + atomicAdd(&A.ctr[C_NEXT], 1ull);
-        }
-        p = __shfl_sync(kFull, p, 0);
-        if (p >= hi) break;
-        const uint64_t e0 = A.eoff[p];
-        const int deg = (int)(A.eoff[p + 1] - e0);
-        if (deg < 3 || deg > 64) continue;  // k_tets_alpha_rows takes the larger balls
-        const uint32_t *N = A.ER + e0;
-        const uint64_t *Lp = A.link + A.loff[p];
-        for (int c = lane; c < deg; c += 32) {
-            const uint32_t x = __ldg(&N[c]);
-            sN[wib][c] = x;
-            sb[wib][c] = __ldg(&A.at[x]);
-            sL[wib][c] = Lp[c];
-        }
-        const Ball B1 = pac::ld_ball(&A.at[p]);
-        const MolGrid G = A.grids[mol_of(A.mol, p)];
-        __syncwarp();
-        for (int a = 0; a < deg - 2; a++)
-            tet_row<V, 1, 64>(A, Q, p, a, deg, 1, sN[wib], sL[wib], sb[wib], sN2[wib], sL2[wib],
-                              smap[wib], B1, G, cand_acc, alpha_acc, tally);
-        __syncwarp();
-    }
-    flush_tally<V>(tally, A.gctr);
-    if (lane == 0) {
-        bump(A.ctr, C_CAND_Q, cand_acc);
-        bump(A.ctr, C_ALPHA_Q, alpha_acc);
-    }
-}
-
-// Work units of k_tets_alpha_rows per ball: ceil((deg - 2) / kUnitRows)
-// groups of rows for a ball with more than 64 upper neighbours, 0 for the
-// others.
-constexpr int kUnitRows = 8;
-__global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, uint32_t *rows) {
-    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const uint64_t deg = eoff[p + 1] - eoff[p];
-    rows[p] = deg > 64 ? (uint32_t)((deg - 2 + kUnitRows - 1) / kUnitRows) : 0u;
-}
-
-// k_tets_alpha_rows: balls of more than 64 upper neighbours, one warp per
-// (ball, group of kUnitRows rows) -- such balls hold many candidates each,
-// and a whole ball per warp left most warps idle behind a few.  uoff[p] is
-// the exclusive prefix of k_heavy_rows; units of the chunk [lo, hi) are
-// handed out from a counter.  Per unit the balls of v1's neighbours beyond
-// its first row are staged.
-template <int V>
-__global__ void __launch_bounds__(128, 6) k_tets_alpha_rows(TetArgs A, TetQueue Q, uint64_t lo,
-                                                            uint64_t hi, const uint64_t *uoff) {
-    __shared__ float4 sb[4][kMaxDeg];
-    __shared__ uint64_t sL2[4][256];  // v2's link rows when they fit (else read in place)
-    __shared__ uint32_t sN2[4][kMaxDeg];
-    __shared__ uint16_t smap[4][kMaxDeg];
-    __shared__ uint32_t sN[4][kMaxDeg];  // v1's upper neighbours (from the unit's first row)
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    unsigned long long cand_acc = 0, alpha_acc = 0;
-    Tally tally;
-    const uint64_t u0 = uoff[lo], u1 = uoff[hi];
+    QRes qr{0, 0};
+    const uint64_t u0 = KW == 1 ? lo : uoff[lo], u1 = KW == 1 ? hi : uoff[hi];
     while (true) {
         uint64_t u = 0;
         if (lane == 0) {
+            // stop handing out work once the queue has overflowed: the chunk
+            // is rerun smaller
             u = (*(volatile unsigned long long *)&A.ctr[C_SURV] > Q.cap)
                     ? u1
                     : u0 + atomicAdd(&A.ctr[C_NEXT], 1ull);
         }
         u = __shfl_sync(kFull, u, 0);
         if (u >= u1) break;
-        // the ball: largest p in [lo, hi) with uoff[p] <= u
-        uint64_t pl = lo, ph = hi;  // uoff[pl] <= u < uoff[ph]
-        while (ph - pl > 1) {
-            const uint64_t mid = (pl + ph) >> 1;
-            if (uoff[mid] <= u) pl = mid;
-            else ph = mid;
+        uint64_t p = u;
+        int a0 = 0;
+        if constexpr (KW != 1) {
+            uint64_t pl = lo, ph = hi;  // uoff[pl] <= u < uoff[ph]
+            while (ph - pl > 1) {
+                const uint64_t mid = (pl + ph) >> 1;
+                if (uoff[mid] <= u) pl = mid;
+                else ph = mid;
+            }
+            p = pl;
+            a0 = (int)(u - uoff[p]) * A.unit_rows;
         }
-        const uint64_t p = pl;
-        const int a0 = (int)(u - uoff[p]) * kUnitRows;
         const uint64_t e0 = A.eoff[p];
         const int deg = (int)(A.eoff[p + 1] - e0);
+        if (KW == 1 && (deg < 3 || deg > 64)) continue;  // the heavy kernel takes the larger balls
         const int W = (deg + 63) >> 6;
-        const uint32_t *N = A.ER + e0;
-        const uint64_t *Lp = A.link + A.loff[p];
+        const uint32_t *Ng = A.ER + e0;
+        const uint64_t *Lg = A.link + A.loff[p];
+        const MolGrid G = A.grids[mol_of(A.mol, p)];
+        const bool refute = A.refute && G.gx <= 16384 && G.gy <= 16384 && G.gz <= 16384;
         for (int c = a0 + lane; c < deg; c += 32) {
-            const uint32_t x = __ldg(&N[c]);
-            sN[wib][c] = x;
-            sb[wib][c] = __ldg(&A.at[x]);
+            const uint32_t x = __ldg(&Ng[c]);
+            S.sN[wib][c] = x;
+            S.sb[wib][c] = __ldg(&A.at[x]);
+            if constexpr (KW == 1) S.sL[wib][c] = Lg[c];
         }
         const Ball B1 = pac::ld_ball(&A.at[p]);
-        const MolGrid G = A.grids[mol_of(A.mol, p)];
         __syncwarp();
-        const int a1 = min(a0 + kUnitRows, deg - 2);
+        const uint64_t *L;
+        if constexpr (KW == 1) L = S.sL[wib];
+        else L = Lg;
+        const int a1 = KW == 1 ? deg - 2 : min(a0 + A.unit_rows, deg - 2);
         for (int a = a0; a < a1; a++)
-            tet_row<V, kMaxW, 256>(A, Q, p, a, deg, W, sN[wib], Lp, sb[wib], sN2[wib], sL2[wib],
-                                   smap[wib], B1, G, cand_acc, alpha_acc, tally);
+            tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, deg, W, L, B1, G, refute, cand_acc,
+                           alpha_acc, kill_acc, ktest_acc, tally);
         __syncwarp();
     }
-    flush_tally<V>(tally, A.gctr);
+    queue_close(Q, qr);
+    // into the chunk's counters: the host adds them to the pass's only when
+    // the chunk is accepted (an overflowing chunk is rerun smaller)
+    flush_tally<V>(tally, A.ctr);
     if (lane == 0) {
         bump(A.ctr, C_CAND_Q, cand_acc);
         bump(A.ctr, C_ALPHA_Q, alpha_acc);
     }
+    kill_acc = warp_sum(kill_acc);
+    ktest_acc = warp_sum(ktest_acc);
+    if (lane == 0) {
+        bump(A.ctr, C_KILLED, kill_acc);
+        bump(A.ctr, C_KTESTS, ktest_acc);
+    }
 }
+
+// Exact-mode tallies and early-refutation counts of an accepted enumeration
+// chunk into the pass's counters.
+__global__ void k_add_tally(const unsigned long long *chunk, unsigned long long *pass) {
+    const int k = threadIdx.x;
+    int which = -1;
+    if (k == 0) which = C_FILTER;
+    else if (k == 1) which = C_FALLBACK;
+    else if (k == 2) which = C_SOS_RANGE;
+    else if (k == 3) which = C_KILLED;
+    else if (k == 4) which = C_KTESTS;
+    if (which >= 0 && chunk[which]) pass[which] += chunk[which];
+}
+
+// Work units of the heavy enumeration per ball: ceil((deg - 2) / unit_rows)
+// groups of rows for a ball with more than 64 upper neighbours, 0 for the
+// others.
+__global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, int unit_rows, uint32_t *rows) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint64_t deg = eoff[p + 1] - eoff[p];
+    rows[p] = deg > 64 ? (uint32_t)((deg - 2 + unit_rows - 1) / unit_rows) : 0u;
+}
+
+constexpr int kScanStep = 4;
 
 // k_tets_scan: the empty-orthosphere test (checkTetsOrthosphere,
 // AlphaComplexLargeData.cu:606-734) of the queued tetrahedra.  Each lane
-// owns one tetrahedron at a time and evaluates two window balls per step; a
-// warp claims kScanClaim queue entries at a time and a lane takes the next
-// unclaimed one as soon as its own is decided.  Survivors are recorded and
-// mark their faces.  COOP (the autotuner's candidates with a hand-off
-// threshold): a tetrahedron still open after A.handoff balls is handed to
-// the cooperative test (the whole warp scans its window); without it the
-// kernel holds fewer registers and runs four blocks per SM.
-template <int V, bool COOP>
-__global__ void __launch_bounds__(256, COOP ? 3 : 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
+// owns one tetrahedron at a time and tests kScanStep window balls per step; a warp
+// claims a range of queue entries at a time and a lane takes the next
+// unclaimed one as soon as its own is decided (claims of A.scan_claim
+// entries: one counter serves every warp).  Each (tetrahedron, ball)
+// decision is taken by the certified filter of certify.cuh when it can
+// prove the reference's binary32 outcome, else by replaying that
+// arithmetic; A.verify replays every certified decision too and counts
+// disagreements (C_CERT_BAD).  Survivors are recorded and mark their faces.
+template <int V>
+__global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
-    __shared__ uint4 lvid[8][kLongCap];
-    __shared__ int4 lcell[8][kLongCap];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
-    unsigned long long evals = 0, oob = 0;
+    unsigned long long evals = 0, oob = 0, certd = 0, bad = 0;
     Tally tally;
     uint64_t head = 0, tail = 0;  // this warp's claimed range (warp-uniform)
     bool have = false, more = true;
     uint32_t p = 0, v2 = 0, v3 = 0, v4 = 0;
-    float pa[3], pb[3], pc[3], pd[3], wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
-    int gX = 0, gY = 0, gZ = 0, q = 0, nev = 0;
-    int4 mycell = make_int4(0, 0, 0, 0);
+    float ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0, cx = 0, cy = 0, cz = 0, dx = 0, dy = 0,
+          dz = 0, wa = 0, wb = 0, wc = 0, wd = 0, orientation = 0;
+    pac::cert::Insphere ct{};
+    int gX = 0, gY = 0, gZ = 0, q = 0;
     uint32_t e = 0, end = 0;
     bool zero = false;
-    int ln = 0;
     const MolGrid *G = A.grids;
-    auto flush_long = [&]() {
-        for (int t = 0; t < ln; t++) {
-            const uint4 vv = lvid[wib][t];
-            const uint32_t p2 = vv.x, u2 = vv.y, u3 = vv.z, u4 = vv.w;
-            const int4 cl = lcell[wib][t];
-            const Ball a1 = pac::ld_ball(&A.at[p2]), a2 = pac::ld_ball(&A.at[u2]),
-                       a3 = pac::ld_ball(&A.at[u3]), a4 = pac::ld_ball(&A.at[u4]);
-            float qa[3], qb[3], qc[3], qd[3];
-            qa[0] = a1.x, qa[1] = a1.y, qa[2] = a1.z;
-            qb[0] = a2.x, qb[1] = a2.y, qb[2] = a2.z;
-            qc[0] = a3.x, qc[1] = a3.y, qc[2] = a3.z;
-            qd[0] = a4.x, qd[1] = a4.y, qd[2] = a4.z;
-            const float xa = wt<V>(a1.r), xb = wt<V>(a2.r), xc = wt<V>(a3.r), xd = wt<V>(a4.r);
-            const float ori = dec_orient<V>(qa, qb, qc, qd, xa, xb, xc, xd, tally);
-            const MolGrid G2 = A.grids[mol_of(A.mol, p2)];
-            int r = coop_test<V>(A, G2, p2, u2, u3, u4, qa, qb, qc, qd, xa, xb, xc, xd, ori, cl, evals,
-                                 tally);
-            if (r != 1 && lane == 0) {
-                const uint32_t *N2 = A.ER + A.eoff[p2];
-                const int deg = (int)(A.eoff[p2 + 1] - A.eoff[p2]);
-                uint32_t dummy = 0;
-                emit_survivor(A, p2, (deg + 63) >> 6, A.loff[p2], N2, key_of(N2, deg, u2, u3, u4),
-                              r == 2, dummy);
-                if (r != 2) atomicAdd(&A.tcount[p2], 1u);
-            }
-        }
-        ln = 0;
-        __syncwarp();
-    };
     while (true) {
         // claim: idle lanes take the next entries of the warp's range
-        unsigned want = __ballot_sync(kFull, !have);
+        const unsigned want = __ballot_sync(kFull, !have);
         if (want && head >= tail && more) {
             uint64_t b = 0;
-            if (lane == 0) b = atomicAdd(claim, (unsigned long long)kScanClaim);
+            if (lane == 0) b = atomicAdd(claim, (unsigned long long)A.scan_claim);
             b = __shfl_sync(kFull, b, 0);
             head = b;
-            tail = min(nq, b + kScanClaim);
+            tail = min(nq, b + (uint64_t)A.scan_claim);
             if (head >= tail) more = false;
         }
         if (want && head < tail) {
-            int r = __popc(want & lt_mask);
+            const int r = __popc(want & lt_mask);
             if (!have && head + r < tail) {
-                uint64_t idx = head + r;
+                const uint64_t idx = head + r;
                 const uint4 vv = Q.vid[idx];
-                int4 cl = Q.cell[idx];
-                p = vv.x;
-                v2 = vv.y;
-                v3 = vv.z;
-                v4 = vv.w;
-                G = A.grids + mol_of(A.mol, p);
-                const Ball a1 = pac::ld_ball(&A.at[p]), a2 = pac::ld_ball(&A.at[v2]),
-                           a3 = pac::ld_ball(&A.at[v3]), a4 = pac::ld_ball(&A.at[v4]);
-                pa[0] = a1.x, pa[1] = a1.y, pa[2] = a1.z, wa = wt<V>(a1.r);
-                pb[0] = a2.x, pb[1] = a2.y, pb[2] = a2.z, wb = wt<V>(a2.r);
-                pc[0] = a3.x, pc[1] = a3.y, pc[2] = a3.z, wc = wt<V>(a3.r);
-                pd[0] = a4.x, pd[1] = a4.y, pd[2] = a4.z, wd = wt<V>(a4.r);
-                orientation = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
-                gX = cl.x;
-                gY = cl.y;
-                gZ = cl.z;
-                mycell = cl;
-                q = 0;
-                nev = 0;
-                zero = false;
-                window_centre(*G, A.cellbeg, cl, e, end, oob);
-                have = true;
+                if (vv.x != kNoTet) {
+                    const float4 sph = Q.sph[idx];
+                    p = vv.x, v2 = vv.y, v3 = vv.z, v4 = vv.w;
+                    G = A.grids + mol_of(A.mol, p);
+                    const Ball a1 = pac::ld_ball(&A.at[p]), a2 = pac::ld_ball(&A.at[v2]),
+                               a3 = pac::ld_ball(&A.at[v3]), a4 = pac::ld_ball(&A.at[v4]);
+                    ax = a1.x, ay = a1.y, az = a1.z, wa = wt<V>(a1.r);
+                    bx = a2.x, by = a2.y, bz = a2.z, wb = wt<V>(a2.r);
+                    cx = a3.x, cy = a3.y, cz = a3.z, wc = wt<V>(a3.r);
+                    dx = a4.x, dy = a4.y, dz = a4.z, wd = wt<V>(a4.r);
+                    {
+                        const float pa[3] = {ax, ay, az}, pb[3] = {bx, by, bz}, pc[3] = {cx, cy, cz},
+                                    pd[3] = {dx, dy, dz};
+                        orientation = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
+                    }
+                    if constexpr (V != pac::kExact)
+                        ct = pac::cert::setup(ax, ay, az, wa, bx, by, bz, wb, cx, cy, cz, wc, dx, dy,
+                                              dz, wd, orientation, sph.x, sph.y, sph.z, G->wmax);
+                    const int4 cl = window_cell(*G, sph.x, sph.y, sph.z);
+                    gX = cl.x, gY = cl.y, gZ = cl.z;
+                    q = 0;
+                    zero = false;
+                    window_centre(*G, A.cellbeg, cl, e, end, oob);
+                    have = true;
+                }
             }
             head = min(tail, head + (uint64_t)__popc(want));
         }
         if (!__any_sync(kFull, have)) {
-            if constexpr (COOP) {
-                if (!more || ln) {
-                    flush_long();
-                    if (!more) break;
-                }
-            } else {
-                if (!more) break;
-            }
+            if (!more) break;
             continue;
         }
-        if constexpr (COOP) {
-            const bool handoff = have && nev >= A.handoff;
-            const unsigned hm = __ballot_sync(kFull, handoff);
-            if (hm) {
-                int pos = ln + __popc(hm & lt_mask);
-                if (handoff && pos < kLongCap) {
-                    lvid[wib][pos] = make_uint4(p, v2, v3, v4);
-                    lcell[wib][pos] = mycell;
-                    have = false;
-                }
-                ln = min(kLongCap, ln + __popc(hm));
-                if (ln > kLongCap - 32) {
-                    __syncwarp();
-                    flush_long();
-                }
-            }
-        }
         if (!have) continue;
-        if constexpr (V != pac::kExact) {
-            // two window balls per step: independent loads and arithmetic
-            // overlap, and the warp-wide bookkeeping above runs half as often
-            if (e < end) {
-                const uint32_t x0 = e, x1 = (e + 1 < end) ? e + 1 : e;
-                const bool ok0 = !(x0 == p || x0 == v2 || x0 == v3 || x0 == v4);
-                const bool ok1 = x1 != x0 && !(x1 == p || x1 == v2 || x1 == v3 || x1 == v4);
-                e = x1 + 1;
-                const Ball b0 = pac::ld_ball(&A.at[x0]), b1 = pac::ld_ball(&A.at[x1]);
-                float pe0[3] = {b0.x, b0.y, b0.z}, pe1[3] = {b1.x, b1.y, b1.z};
-                const float r0 = dec_insphere<V>(pa, pb, pc, pd, pe0, wa, wb, wc, wd, wt<V>(b0.r), tally);
-                const float r1 = dec_insphere<V>(pa, pb, pc, pd, pe1, wa, wb, wc, wd, wt<V>(b1.r), tally);
-                evals += (int)ok0 + (int)ok1;
-                nev += (int)ok0 + (int)ok1;
-                const bool viol = (ok0 && (orientation < 0 ? (r0 < 0) : (r0 > 0))) ||
-                                  (ok1 && (orientation < 0 ? (r1 < 0) : (r1 > 0)));
-                if (viol) {
-                    have = false;
-                    continue;
-                }
-                if ((ok0 && r0 == 0) || (ok1 && r1 == 0)) zero = true;
-                continue;
-            }
-        } else {
-            if (e < end) {
-                uint32_t x = e++;
-                if (x == p || x == v2 || x == v3 || x == v4) continue;
-                const Ball atom = pac::ld_ball(&A.at[x]);
-                float pe[3];
-                pe[0] = atom.x, pe[1] = atom.y, pe[2] = atom.z;
-                float we = wt<V>(atom.r);
+        if (e < end) {
+            // kScanStep window balls per step: their loads overlap, and the
+            // warp-wide bookkeeping above runs once per step
+            const uint32_t cnt = min(end - e, (uint32_t)kScanStep);
+            Ball bq[kScanStep];
+#pragma unroll
+            for (int t = 0; t < kScanStep; t++)
+                bq[t] = pac::ld_ball(&A.at[e + min((uint32_t)t, cnt - 1)]);
+            const uint32_t x0 = e;
+            e += cnt;
+            bool viol = false;
+#pragma unroll
+            for (int t = 0; t < kScanStep; t++) {
+                const uint32_t x = x0 + t;
+                const Ball bb = bq[t];
+                if ((uint32_t)t >= cnt || viol || x == p || x == v2 || x == v3 || x == v4) continue;
+                const float we = wt<V>(bb.r);
+                int dec = -1;
+                if constexpr (V != pac::kExact) dec = pac::cert::test(ct, bb.x, bb.y, bb.z, we);
                 evals++;
-                nev++;
-                float result = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
-                bool viol = orientation < 0 ? (result < 0) : (result > 0);
-                if (viol) {
-                    have = false;
-                    continue;
+                if (dec >= 0) certd++;
+                if (dec < 0 || A.verify) {
+                    const float pa[3] = {ax, ay, az}, pb[3] = {bx, by, bz}, pc[3] = {cx, cy, cz},
+                                pd[3] = {dx, dy, dz}, pe[3] = {bb.x, bb.y, bb.z};
+                    const float res =
+                        dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd, we, tally);
+                    const int rdec = (orientation < 0 ? (res < 0) : (res > 0)) ? 1 : 0;
+                    if (dec >= 0 && dec != rdec) bad++;
+                    if (dec < 0) {
+                        dec = rdec;
+                        if (res == 0) zero = true;
+                    }
                 }
-                if (result == 0) zero = true;
-                continue;
+                viol = dec == 1;
             }
+            if (viol) have = false;
+            continue;
         }
         bool found = false;
         while (q < kWindowParts && !found) found = window_part(*G, A.cellbeg, gX, gY, gZ, q++, e, end);
         if (!found) {
-            const uint32_t *N = A.ER + A.eoff[p];
-            const int deg = (int)(A.eoff[p + 1] - A.eoff[p]);
-            uint32_t dummy = 0;
-            emit_survivor(A, p, (deg + 63) >> 6, A.loff[p], N, key_of(N, deg, v2, v3, v4), zero,
-                          dummy);
-            if (!zero) atomicAdd(&A.tcount[p], 1u);
+            emit_survivor(A.eoff, A.ER, A.loff, A.faces, A.surv, A.surv_cap, A.pend, A.pend_cap,
+                          A.ctr, A.tcount, p, v2, v3, v4, zero);
             have = false;
         }
     }
     evals = warp_sum(evals);
     oob = warp_sum(oob);
+    certd = warp_sum(certd);
+    bad = warp_sum(bad);
     flush_tally<V>(tally, A.ctr);
     if (lane == 0) {
         bump(A.ctr, C_INSPHERE, evals);
         bump(A.ctr, C_OOB, oob);
+        bump(A.ctr, C_CERT, certd);
+        bump(A.ctr, C_CERT_BAD, bad);
     }
 }
 
@@ -1901,6 +1998,20 @@ __global__ void k_mol_rows(uint32_t n_mol, const uint64_t *ball_off, uint64_t n,
 }
 
 // ------------------------------------------------------------------ host
+// The enumeration kernels' shared memory exceeds the static 48 KB: allow it
+// (once per device and flavour; the attribute belongs to the kernel).
+template <int V>
+static int enum_smem_optin(pac::Ctx &ctx) {
+    static bool done[64] = {};
+    if (ctx.device >= 0 && ctx.device < 64 && done[ctx.device]) return PAC_OK;
+    CK(cudaFuncSetAttribute(k_tets_enum<V, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(EnumSmem<1>)));
+    CK(cudaFuncSetAttribute(k_tets_enum<V, kMaxW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(EnumSmem<kMaxW>)));
+    if (ctx.device >= 0 && ctx.device < 64) done[ctx.device] = true;
+    return PAC_OK;
+}
+
 struct Timer {
     pac::Ctx &ctx;
     int i = 0;
@@ -1963,7 +2074,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     }
     k_bbox<<<blocks_for(n, 256), 256, 0, s>>>(in.d_balls, n, mol, mm);
     LAUNCH_CHECK(ctx);
-    k_grid<<<blocks_for(nm, 128), 128, 0, s>>>(mm, nm, in.alpha, grids, ncell_d);
+    k_grid<<<blocks_for(nm, 128), 128, 0, s>>>(mm, nm, in.sol, in.alpha, grids, ncell_d);
     LAUNCH_CHECK(ctx);
     std::vector<MolGrid> hg(nm);
     CK(cudaMemcpyAsync(hg.data(), grids, sizeof(MolGrid) * nm, cudaMemcpyDeviceToHost, s));
@@ -2063,8 +2174,11 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     T.grids = grids;
     T.alpha = in.alpha;
     T.ctr = ctr;
-    T.gctr = ctr;
-    T.handoff = std::max(1, cfg.handoff);
+    T.cellof = cellof;
+    T.refute = cfg.refute ? 1 : 0;
+    T.verify = cfg.verify ? 1 : 0;
+    T.unit_rows = std::max(1, cfg.unit_rows);
+    T.scan_claim = std::max(32, cfg.scan_claim);
     T.tcount = ar.alloc_n<uint32_t>(n);
     uint64_t *toff = ar.alloc_n<uint64_t>(n + 1);
     if (!T.tcount || !toff) return PAC_ERR_OOM;
@@ -2090,7 +2204,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         const uint64_t qcap = std::max<uint64_t>(1 << 16, cfg.queue_entries);
         TetQueue Q;
         Q.vid = ar.alloc_n<uint4>(qcap);
-        Q.cell = ar.alloc_n<int4>(qcap);
+        Q.sph = ar.alloc_n<float4>(qcap);
         Q.cap = qcap;
         uint64_t scap = std::max<uint64_t>(1024, 16 * n);
         T.surv = ar.alloc_n<uint2>(scap);
@@ -2099,7 +2213,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         T.pend_cap = scap / 4 + 1024;
         unsigned long long *claim = ar.alloc_n<unsigned long long>(1);
         unsigned long long *ctrA = ar.alloc_n<unsigned long long>(C_NCOUNTERS);
-        if (!Q.vid || !Q.cell || !T.surv || !T.pend || !claim || !ctrA) return PAC_ERR_OOM;
+        if (!Q.vid || !Q.sph || !T.surv || !T.pend || !claim || !ctrA) return PAC_ERR_OOM;
         CK(cudaMemsetAsync(ctr + C_SURV, 0, 2 * sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(ctr + C_INSPHERE, 0, sizeof(unsigned long long), s));
         CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
@@ -2110,31 +2224,37 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         if (!hrows || !uoff) return PAC_ERR_OOM;
         uint64_t heavy_units = 0;
         if (maxdeg > 64) {
-            k_heavy_rows<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, hrows);
+            k_heavy_rows<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, T.unit_rows, hrows);
             LAUNCH_CHECK(ctx);
             rc = exclusive_scan(ctx, hrows, n, uoff);
             if (rc) return rc;
             CK(cudaMemcpyAsync(&heavy_units, uoff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
         }
+        rc = enum_smem_optin<V>(ctx);
+        if (rc) return rc;
         unsigned long long cand_total = 0, alpha_total = 0;
         uint64_t lo = 0, chunk = n;
         // verbose: per-chunk enumeration and scan times
         cudaEvent_t vev[3] = {nullptr, nullptr, nullptr};
         if (cfg.verbose)
             for (auto &e : vev) CK(cudaEventCreate(&e));
+        const unsigned enum_blocks = 148u * (unsigned)std::max(1, cfg.enum_blocks);
+        const unsigned heavy_blocks = 148u * (unsigned)std::max(1, cfg.heavy_blocks);
         while (lo < n) {
             const uint64_t hi = std::min<uint64_t>(n, lo + chunk);
             TetArgs TA = T;
             TA.ctr = ctrA;
             if (cfg.verbose) CK(cudaEventRecord(vev[0], s));
             CK(cudaMemsetAsync(ctrA, 0, sizeof(unsigned long long) * C_NCOUNTERS, s));
-            k_tets_alpha1<V><<<std::min<unsigned>(warp_blocks(hi - lo), 148 * 4), 256, 0, s>>>(
-                TA, Q, lo, hi);
+            k_tets_enum<V, 1><<<(unsigned)std::min<uint64_t>(enum_blocks, (hi - lo + 7) / 8),
+                                EnumSmem<1>::kWarps * 32, sizeof(EnumSmem<1>), s>>>(TA, Q, lo, hi,
+                                                                                   nullptr);
             LAUNCH_CHECK(ctx);
             if (heavy_units) {  // balls with more than 64 upper neighbours, by rows
                 CK(cudaMemsetAsync(ctrA + C_NEXT, 0, sizeof(unsigned long long), s));
-                k_tets_alpha_rows<V><<<148 * 6, 128, 0, s>>>(TA, Q, lo, hi, uoff);
+                k_tets_enum<V, kMaxW><<<heavy_blocks, EnumSmem<kMaxW>::kWarps * 32,
+                                        sizeof(EnumSmem<kMaxW>), s>>>(TA, Q, lo, hi, uoff);
                 LAUNCH_CHECK(ctx);
             }
             if (cfg.verbose) CK(cudaEventRecord(vev[1], s));
@@ -2174,14 +2294,15 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             }
             cand_total += ha[C_CAND_Q];
             alpha_total += ha[C_ALPHA_Q];
+            if (ha[C_FILTER] || ha[C_FALLBACK] || ha[C_SOS_RANGE] || ha[C_KILLED] || ha[C_KTESTS]) {
+                k_add_tally<<<1, 32, 0, s>>>(ctrA, ctr);
+                LAUNCH_CHECK(ctx);
+            }
             CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
-            if (cfg.handoff < (1 << 30))
-                k_tets_scan<V, true><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued,
-                                                                                     claim);
-            else
-                k_tets_scan<V, false><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued,
-                                                                                      claim);
-            LAUNCH_CHECK(ctx);
+            if (queued) {
+                k_tets_scan<V><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued, claim);
+                LAUNCH_CHECK(ctx);
+            }
             if (cfg.verbose) {
                 float me = 0.f, ms = 0.f;
                 CK(cudaEventRecord(vev[2], s));
@@ -2190,9 +2311,9 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                 CK(cudaEventElapsedTime(&ms, vev[1], vev[2]));
                 std::fprintf(stderr,
                              "[pac] tetrahedra of balls [%llu, %llu): %llu candidates, %llu alpha, "
-                             "%llu queued; enumeration %.3f ms, scan %.3f ms\n",
+                             "%llu refuted early, %llu queued; enumeration %.3f ms, scan %.3f ms\n",
                              (unsigned long long)lo, (unsigned long long)hi, ha[C_CAND_Q],
-                             ha[C_ALPHA_Q], queued, me, ms);
+                             ha[C_ALPHA_Q], ha[C_KILLED], queued, me, ms);
             }
             // next chunk sized from this one's queue fill
             if (queued)
@@ -2329,6 +2450,10 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         st->sos_calls = hc[C_SOS];
         st->filter_evals = hc[C_FILTER];
         st->exact_fallbacks = hc[C_FALLBACK];
+        st->early_refuted = hc[C_KILLED];
+        st->early_tests = hc[C_KTESTS];
+        st->cert_decisions = hc[C_CERT];
+        st->cert_disagreements = hc[C_CERT_BAD];
         st->ortho_out_of_grid = hc[C_OOB];
         st->max_degree = maxdeg;
         st->ms_grid = tm.ms(0, 1);

@@ -30,6 +30,16 @@ __device__ __forceinline__ Ball ld_ball(const float4 *p) {
 // formula sets; kExact selects the decision-exact predicates (exactpred.cuh)
 enum : int { kUpstream = 0, kPlainXmp = 1, kExact = 2 };
 
+// The reference compares binary32 results in double precision: THRES and
+// ATHRES are the double literal 0.0 (LD:48-49), so `x <= (alpha + ATHRES)`
+// (LD:185, 347, 588) and `powDist + THRES <= currentDist` (LD:829, 968)
+// convert their binary32 operands to double.  That conversion is exact and
+// adding +0.0 changes no value a comparison sees, so each such test has the
+// outcome of the binary32 comparison x <= y, NaNs included; that is what is
+// evaluated here.  (Tests whose right-hand side is a double product, in the
+// plain-xmp formulas, stay in double.)
+__device__ __forceinline__ bool le_as_double(float x, float y) { return x <= y; }
+
 // markRealEdges: LD:173-189 (upstream) / PLAIN:209-229 (plain-xmp).
 template <int V>
 __device__ __forceinline__ bool edge_alpha(const Ball a1, const Ball a2, float alpha) {
@@ -42,7 +52,7 @@ __device__ __forceinline__ bool edge_alpha(const Ball a1, const Ball a2, float a
     float t = (d - a * a1.x - b * a1.y - c * a1.z);
     if (V == kUpstream) {
         float currentDist = ((t * t) / (a * a + b * b + c * c)) - (a1.r * a1.r);
-        return currentDist <= ((double)alpha + 0.0);
+        return le_as_double(currentDist, alpha);
     } else {
         float currentDistTerm = ((t * t)) - (a1.r * a1.r) * (a * a + b * b + c * c);
         return currentDistTerm <= ((double)alpha + 0.0) * (a * a + b * b + c * c);
@@ -89,7 +99,7 @@ __device__ __forceinline__ bool tri_alpha(const Ball a1, const Ball a2, const Ba
         float dist = (a1.x - X) * (a1.x - X) + (a1.y - Y) * (a1.y - Y) +
                      (a1.z - Z) * (a1.z - Z) - a1.r * a1.r;
         ortho = make_float4(X, Y, Z, dist);
-        return dist <= ((double)alpha + 0.0);
+        return le_as_double(dist, alpha);
     } else {
         D = D * 2;
         float X = Dx;
@@ -146,7 +156,7 @@ __device__ __forceinline__ bool tet_alpha(const Ball a1, const Ball a2, const Ba
     float dist = (a2.x - X) * (a2.x - X) + (a2.y - Y) * (a2.y - Y) + (a2.z - Z) * (a2.z - Z) -
                  a2.r * a2.r;
     ortho = make_float4(X, Y, Z, dist);
-    return dist <= ((double)alpha + 0.0);
+    return le_as_double(dist, alpha);
 }
 
 // orient3d determinant (PRED:2015-2045); the error bound there is dead.
@@ -230,7 +240,7 @@ __device__ __forceinline__ bool attached(const Ball e, float px, float py, float
                                          float currentDist) {
     float powDist = (e.x - px) * (e.x - px) + (e.y - py) * (e.y - py) +
                     (e.z - pz) * (e.z - pz) - (e.r * e.r);
-    return powDist + 0.0 <= currentDist;
+    return le_as_double(powDist, currentDist);
 }
 
 // Foot of the radical plane of an edge and its power (LD:936-949).

@@ -332,9 +332,19 @@ int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uin
     for (int k = 0; k < 4; k++) nblocks += (counts[k] + 127) / 128;
     double4 *partial = ctx.arena.alloc_n<double4>(nblocks);
     if (!acc || !partial || (grad && (!dV || !dA))) return PAC_ERR_OOM;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    // two timing events, destroyed on every return path
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        Events() {
+            cudaEventCreate(&e[0]);
+            cudaEventCreate(&e[1]);
+        }
+        ~Events() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[1];
     cudaEventRecord(e0, s);
     if (grad) {
         cudaMemsetAsync(dV, 0, 4 * sizeof(double) * n, s);
@@ -351,15 +361,18 @@ int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uin
     }
     pac_union::k_union_total<<<1, 256, 0, s>>>(partial, off, acc);
     ctx.launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(s);  // the launches that did start finish first
+        return set_error(PAC_ERR_CUDA, std::string("union measure launch: ") + cudaGetErrorString(e));
+    }
     cudaEventRecord(e1, s);
     double h[2];
     cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
         return set_error(PAC_ERR_CUDA, std::string("union measure: ") + cudaGetErrorString(e));
     if (ms) cudaEventElapsedTime(ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (vol) *vol = h[0];
     if (area) *area = h[1];
     return PAC_OK;
@@ -426,6 +439,15 @@ extern "C" int pac_union_measure_noalloc(pac_ctx *ctx, const double *d_xyzr, uin
     if ((d_dvol == nullptr) != (d_darea == nullptr))
         return pac::set_error(PAC_ERR_INVALID_ARG,
                               "pass both gradient buffers or neither (nothing is allocated)");
+    // The kernels read the lists in place: they must be device lists of this
+    // many balls (host lists would be dereferenced as device addresses).
+    if (cx->on_device != 1)
+        return pac::set_error(PAC_ERR_INVALID_ARG,
+                              "pac_union_measure_noalloc needs device lists (on_device = 1)");
+    if (cx->n_vertices && cx->n_vertices != n)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "complex and balls differ in size");
+    if ((cx->n_edges && !cx->edges) || (cx->n_tris && !cx->tris) || (cx->n_tets && !cx->tets))
+        return pac::set_error(PAC_ERR_INVALID_ARG, "a non-empty list has a null pointer");
     const uint32_t *lists[4] = {nullptr, cx->edges, cx->tris, cx->tets};
     const uint64_t counts[4] = {n, cx->n_edges, cx->n_tris, cx->n_tets};
     uint64_t blocks = 0;

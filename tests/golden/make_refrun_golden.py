@@ -129,4 +129,6 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "refrun"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_refrun_golden.py OUTDIR")
+    main(sys.argv[1])

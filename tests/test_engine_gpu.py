@@ -337,5 +337,78 @@ def test_autotuner_passes_all_give_the_same_lists(pac, orc):
     with pac.Engine(autotune=True) as eng:
         for _ in range(10):  # 8 candidate shapes, then the chosen one
             _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
-    with pac.Engine(handoff=3, scan_blocks=2) as eng:
+    with pac.Engine(enum_blocks=2, scan_blocks=2, heavy_blocks=3, unit_rows=3, scan_claim=64) as eng:
         _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint32).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("refute", [True, False])
+def test_headline_100k_matches_restatement_digest(pac, refute):
+    """The workload the bench's headline is quoted on: the 100,000-ball
+    globule plus 8 corner balls, sol 1.4, alpha 1, upstream formulas, as
+    written, strict -- lists in reference order and the six stage counters
+    against the restatement's digests (tests/golden/make_headline_digest.py),
+    with and without the enumeration's early refutation."""
+    import hashlib
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "headline_100k.json")))
+    balls = pac.pad_corners(pac.globule(100_000, seed=pac.SEED_BASE + 4))
+    assert hashlib.sha256(balls.tobytes()).hexdigest() == man["input_sha256"]
+    with pac.Engine(tet_mode="as-written", refute=refute) as eng:
+        r = eng.alpha_complex(balls, 1.4, 1.0)
+    assert [len(r.edges), len(r.tris), len(r.tets)] == man["counts"]
+    assert [_sha(r.edges), _sha(r.tris), _sha(r.tets)] == man["sha256"]
+    for k, v in man["stats"].items():
+        assert r.stats[k] == v, k
+    if refute:
+        # most alpha tetrahedra never reach the queue
+        assert r.stats["early_refuted"] > 0.5 * r.stats["alpha_tets"]
+    else:
+        assert r.stats["early_refuted"] == 0
+
+
+def test_certified_filter_agrees_with_replay_on_gpu(pac):
+    """Verify mode: the scan replays the reference's binary32 insphere for
+    every decision the certified filter takes and counts disagreements --
+    on a generic globule and on lattice-snapped inputs (exact ties)."""
+    for balls in (pac.globule(20_000, seed=pac.SEED_BASE + 4),
+                  pac.snapped_globule(5_000, seed=pac.SEED_BASE + 1)):
+        with pac.Engine(tet_mode="as-written", verify=True, refute=False) as eng:
+            r = eng.alpha_complex(balls, 1.4, 1.0)
+        st = r.stats
+        print("certified %d of %d insphere decisions, %d disagreements"
+              % (st["cert_decisions"], st["insphere_evals"], st["cert_disagreements"]))
+        assert st["cert_disagreements"] == 0
+        assert st["cert_decisions"] > 0.9 * st["insphere_evals"]
+
+
+@pytest.mark.slow
+def test_batch_4096_matches_restatement_digests(pac):
+    """The batched configuration in full: 4,096 molecules of log-uniform
+    size in [200, 20000] (17.47 M balls), sol 1.4, alpha 0.5, as written, in
+    one pac_alpha_complex_batch call; every molecule's lists against the
+    restatement's (tests/golden/batch_4096.json: per-molecule list lengths
+    and a sha256 per list kind over all molecules in order)."""
+    import hashlib
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "batch_4096.json")))
+    sizes = pac.batch_sizes(4096)
+    balls, off = pac.batch(sizes)
+    assert hashlib.sha256(balls.tobytes()).hexdigest() == man["input_sha256"]
+    with pac.Engine(tet_mode="as-written") as eng:
+        res, st = eng.alpha_complex_batch(balls, off, 1.4, 0.5)
+    got = np.array([r.counts() for r in res], dtype=np.int64)
+    want = np.stack([man["edges_per_molecule"], man["tris_per_molecule"],
+                     man["tets_per_molecule"]], 1)
+    bad = np.nonzero((got != want).any(1))[0]
+    assert len(bad) == 0, "molecules with other list lengths: %s" % bad[:10]
+    h = [hashlib.sha256() for _ in range(3)]
+    for r in res:
+        for k, a in enumerate((r.edges, r.tris, r.tets)):
+            h[k].update(np.ascontiguousarray(a, dtype=np.uint32).tobytes())
+    assert [x.hexdigest() for x in h] == man["sha256_concat"]
+    print("batch of 4,096: %d simplices, %.0f ms" % (got.sum(), st["ms_total"]))

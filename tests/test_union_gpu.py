@@ -144,3 +144,37 @@ def test_union_gradient_fd_100k_1000_coordinates(pac):
     assert np.median(lv_) < 1e-8 and np.median(la_) < 1e-8
     assert np.quantile(lv_, 0.99) < 1e-6 and np.quantile(la_, 0.99) < 1e-6
     assert lv_.max() < 1e-4 and la_.max() < 1e-4
+
+
+def test_repeated_measure_calls_do_not_grow_device_memory(pac):
+    """Each union-measure call copies its inputs and takes its scratch from
+    the context's pool and gives them back on return: a loop of a few
+    hundred calls (an optimisation or finite-difference loop) leaves the
+    device memory in use flat after the first calls."""
+    import torch
+    balls = pac.globule(1500, seed=34)
+    x = pac.grown_radii(balls, SOL, ALPHA)
+    with pac.Engine(tet_mode="as-written") as eng:
+        r = eng.alpha_complex(balls, SOL, ALPHA)
+        d = torch.from_numpy(balls).cuda()
+        dx = torch.from_numpy(x).cuda()
+        dv = torch.empty_like(dx)
+        da = torch.empty_like(dx)
+        torch.cuda.synchronize()
+        cx, _ = eng.alpha_complex_device(d.data_ptr(), len(balls), SOL, ALPHA)
+        for _ in range(3):  # warm: the pool reaches its size for this work
+            eng.union_measure(x, r, grad=True)
+            eng.union_measure_device(dx.data_ptr(), len(balls), cx, dv.data_ptr(), da.data_ptr())
+            eng.union_measure_device(dx.data_ptr(), len(balls), cx)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        first = eng.union_measure_device(dx.data_ptr(), len(balls), cx)
+        for _ in range(300):
+            eng.union_measure(x, r, grad=True)
+            eng.union_measure_device(dx.data_ptr(), len(balls), cx, dv.data_ptr(), da.data_ptr())
+            got = eng.union_measure_device(dx.data_ptr(), len(balls), cx)
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
+        # the device complex is still the one computed before the loop
+        assert got == first
+    assert free0 - free1 < (64 << 20), (free0, free1)

@@ -45,11 +45,50 @@ def test_noalloc_matches_allocating_entry_point_twice(pac):
 
 def test_noalloc_rejects_oversized_complex(pac):
     """Beyond the fixed scratch (65,536 blocks of 128 simplices) the call
-    fails before running anything."""
+    fails before running anything.  The complex is backed by real zeroed
+    device buffers, so that even a launch would read valid memory."""
+    import torch
+    n = 16
+    x = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
+    tets = torch.zeros(4 * 9_000_000, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
     with pac.Engine() as eng:
-        cx = pac.Complex(16, 1, 0, 0, 9_000_000, None, None,
-                         ctypes.cast(ctypes.c_void_p(16), ctypes.POINTER(ctypes.c_uint32)))
+        cx = pac.Complex(n, 1, 0, 0, 9_000_000, None, None,
+                         ctypes.cast(ctypes.c_void_p(tets.data_ptr()),
+                                     ctypes.POINTER(ctypes.c_uint32)))
         with pytest.raises(pac.PacError) as ei:
-            eng.union_measure_noalloc(16, 16, cx)
+            eng.union_measure_noalloc(x.data_ptr(), n, cx)
         assert ei.value.status == -3
         assert "65536" in str(ei.value)
+
+
+def test_noalloc_rejects_host_lists_and_size_mismatch(pac):
+    """The kernels read the lists in place, so a complex with host lists
+    (on_device 0 or 3) or one built for another number of balls is refused
+    with an invalid-argument status before anything is launched: the host
+    pointers below are never handed to a kernel."""
+    import torch
+    n = 8
+    x = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    host_tets = np.zeros((3, 4), np.uint32)
+    ptr = host_tets.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+    with pac.Engine() as eng:
+        for kind in (0, 3):
+            cx = pac.Complex(n, kind, 0, 0, 3, None, None, ptr)
+            with pytest.raises(pac.PacError) as ei:
+                eng.union_measure_noalloc(x.data_ptr(), n, cx)
+            assert ei.value.status == -1 and "device lists" in str(ei.value)
+        dev_tets = torch.zeros(12, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        cx = pac.Complex(n + 5, 1, 0, 0, 3, None, None,
+                         ctypes.cast(ctypes.c_void_p(dev_tets.data_ptr()),
+                                     ctypes.POINTER(ctypes.c_uint32)))
+        with pytest.raises(pac.PacError) as ei:
+            eng.union_measure_noalloc(x.data_ptr(), n, cx)
+        assert ei.value.status == -1 and "differ in size" in str(ei.value)
+        # a non-empty list without a pointer
+        cx = pac.Complex(n, 1, 0, 0, 3, None, None, None)
+        with pytest.raises(pac.PacError) as ei:
+            eng.union_measure_noalloc(x.data_ptr(), n, cx)
+        assert ei.value.status == -1
