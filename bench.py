@@ -132,9 +132,7 @@ def cpu_baseline(threads):
             "sample": "%d-ball globule, sol 1.4, alpha 1.0, as-written, %.2f s" % (CPU_SAMPLE, dt)}
 
 
-REF_EXE = os.path.join(ROOT, "oracle", "_ref", "parallelac-largeData-rr128-nofma")
-REF_SAMPLE = 25_000
-REF_WARM = 1_300
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def config_of(n):
@@ -145,111 +143,106 @@ def config_of(n):
             "l2": "flushed between steps (256 MB write)"}
 
 
-def _ref_run(exe, balls, tmp):
-    """One run of the reference binary: CRD in, output file out; returns its
-    own 'Total time taken (ms)' figure, the wall time and the counts line of
-    the file it wrote."""
-    import re
-    crd, out = os.path.join(tmp, "in.crd"), os.path.join(tmp, "out.txt")
-    with open(crd, "w") as f:
-        f.write("%d\n" % len(balls))
-        for r in balls:
-            f.write("%r %r %r %r\n" % tuple(float(v) for v in r))
-    t0 = time.perf_counter()
-    p = subprocess.run([exe, crd, out, repr(SOL), repr(ALPHA), str(len(balls))],
-                       capture_output=True, text=True, errors="replace", timeout=900)
-    wall = time.perf_counter() - t0
-    m = re.search(r"Total time taken \(ms\):\s*([0-9.]+)", p.stdout)
-    if p.returncode != 0 or not m:
-        raise RuntimeError("reference run failed (rc %d): %s" % (p.returncode, p.stdout[-300:]))
-    with open(out) as f:
-        counts = [int(v) for v in f.readline().split()]
-    return float(m.group(1)), wall, counts
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint32).tobytes()).hexdigest()
+
+
+def _golden(name):
+    p = os.path.join(GOLDEN, name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+def reference_binary_record():
+    """The reference binary's own run on the full headline workload (one run,
+    tests/golden/refrun/refrun_manifest.json, case glob100k_s14_a1, recorded
+    by tests/golden/make_refrun_golden.py on a B200)."""
+    man = _golden(os.path.join("refrun", "refrun_manifest.json")) or {}
+    rec = man.get("glob100k_s14_a1", {}).get("builds", {}).get("rr128-nofma")
+    if not rec or rec.get("rc") != 0:
+        return None
+    head = _golden("headline_100k.json") or {}
+    return {"binary": "parallelac-largeData built with -maxrregcount=128 -fmad=false",
+            "n_balls": man["glob100k_s14_a1"]["n"], "total_ms": rec.get("total_ms"),
+            "wall_s": rec.get("wall_s"),
+            "balls_per_s": man["glob100k_s14_a1"]["n"] / (rec["total_ms"] / 1e3)
+            if rec.get("total_ms") else None,
+            "lists_equal_headline_digest": rec.get("sha256") == head.get("sha256"),
+            "on": "one B200, recorded once (tests/golden/refrun/refrun_manifest.json)"}
 
 
 def run_reference(args):
-    """The reference arm.  The reference is a CUDA program: its own
-    AlphaComplexLargeData.cu, compiled from its sources by oracle/ref_build.sh
-    with -maxrregcount=128 (built as its CMakeLists.txt says, its orthosphere
-    kernel cannot launch on this GPU and the program aborts) and -fmad=false
-    (so that it computes the same bit-exact complex as this workload), run on
-    the same GPU.  One step = one run of the binary on a 25,000-ball globule
-    sample of the workload (same generator, density, radii, sol-rad, alpha,
-    corner padding); its cost grows slower than linearly with size, so a
-    sample understates its throughput on the full 100k workload somewhat.
-    Before the runs the oracle checks that the sample is one the reference
-    handles safely (every orthosphere window centre inside its grid; no two
-    equal weighted points, on which its simulation of simplicity never ends)
-    and gives the counts that the reference's output must have.  Without the
-    binary (no reference tree where it was built) the oracle port is timed on
-    the host cores instead."""
+    """The reference arm.  The reference (AlphaComplexLargeData.cu) is a CUDA
+    program with no CPU implementation of the path; its arithmetic and
+    decision procedure are restated on the CPU by the oracle
+    (oracle/pac_oracle.c, pinned to the reference binary's own outputs), and
+    that port is what this arm times: the whole 100,008-ball workload per
+    step, all host threads, the same config, metric and unit as the GPU arm.
+    The input comes from the oracle library's copy of the workload generator
+    (no library of the product is loaded).  The reference binary itself,
+    run once on the same workload on a B200 (a few minutes per run), is
+    reported beside it as `reference_binary`."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    pac = ge.load_package()
     orc = ge.load_oracle()
-    base = {"impl": "reference", "metric": METRIC, "unit": "balls/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_of(N_BALLS + 8)}
-    if os.path.exists(REF_EXE):
-        balls = pac.pad_corners(pac.globule(REF_SAMPLE, seed=pac.SEED_BASE + 4))
-        warm = pac.pad_corners(pac.globule(REF_WARM, seed=pac.SEED_BASE))
-        want = {}
-        for name, b in (("sample", balls), ("warm", warm)):
-            e, t, q, st = orc.alpha_complex(b, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True,
-                                            threads=threads)
-            if st["ortho_out_of_grid"] or len(np.unique(b, axis=0)) != len(b):
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  "sample outside what the reference handles safely"}))
-                return 0
-            want[name] = [len(b), len(e), len(t), len(q)]
-        with tempfile.TemporaryDirectory() as tmp:
-            for _ in range(args.warmup):
-                _, _, c = _ref_run(REF_EXE, warm, tmp)
-                assert c == want["warm"], (c, want["warm"])
-            ms, walls = [], []
-            for _ in range(args.steps):
-                t, w, c = _ref_run(REF_EXE, balls, tmp)
-                assert c == want["sample"], (c, want["sample"])
-                ms.append(t)
-                walls.append(w)
-        per = sum(ms) / len(ms)
-        v = len(balls) / (per / 1e3)
-        sample = ("%d-ball globule + 8 corner balls per step, one run of the reference "
-                  "binary (-maxrregcount=128 -fmad=false) on this GPU; its own 'Total time "
-                  "taken' (input copy, all kernels, output copy); warm-up runs on a %d-ball "
-                  "globule" % (REF_SAMPLE, REF_WARM))
-        line = dict(base, value=v, ms_per_step=per,
-                    cpu_baseline={"value": v, "unit": "balls/s", "cores": 1,
-                                  "kind": "reference", "sample": sample},
-                    e2e={"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
-                         "d2h_bytes_per_step": 0},
-                    reference={"binary": os.path.basename(REF_EXE), "on": "gpu",
-                               "counts_match_oracle": True, "counts": want["sample"][1:],
-                               "wall_s_per_step": sum(walls) / len(walls)})
-        print(json.dumps(line), flush=True)
-        return 0
-
-    balls = pac.globule(CPU_SAMPLE, seed=pac.SEED_BASE + 4)
+    balls = orc.pad_corners(orc.globule(N_BALLS, seed=orc.SEED_BASE + 4))
+    n = len(balls)
+    head = _golden("headline_100k.json")
+    # the restatement has no warm-up effects beyond page faults: one untimed
+    # run whatever W is, so that the arm ends within minutes
     for _ in range(min(args.warmup, 1)):
-        orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
-    t = []
+        e, t, q, _ = orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True,
+                                       threads=threads)
+    times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True, threads=threads)
-        t.append(time.perf_counter() - t0)
-    per = sum(t) / len(t)
-    v = CPU_SAMPLE / per
-    sample = "%d-ball globule per step, oracle port on %d host threads" % (CPU_SAMPLE, threads)
-    line = dict(base, value=v, ms_per_step=per * 1e3,
-                cpu_baseline={"value": v, "unit": "balls/s", "cores": threads, "kind": "port",
-                              "sample": sample},
-                e2e={"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
-                     "d2h_bytes_per_step": 0})
+        e, t, q, _ = orc.alpha_complex(balls, SOL, ALPHA, orc.UPSTREAM, tet_ortho=True,
+                                       threads=threads)
+        times.append(time.perf_counter() - t0)
+    per = sum(times) / len(times)
+    v = n / per
+    parity = bool(head) and [_sha(e), _sha(t), _sha(q)] == head["sha256"]
+    sample = ("the full %d-ball workload per step (CPU restatement of the reference, "
+              "%d host threads)" % (n, threads))
+    line = {"impl": "reference", "metric": METRIC, "unit": "balls/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": min(args.warmup, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(n), "value": v, "ms_per_step": per * 1e3,
+            "cpu_baseline": {"value": v, "unit": "balls/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "balls/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "parity": {"headline_100k": parity},
+            "reference_binary": reference_binary_record()}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _device_lists(cx):
+    """Host copies of a device complex's three lists (through torch)."""
+    import ctypes
+    import torch
+
+    class _View:
+        def __init__(self, ptr, count):
+            self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4",
+                                             "data": (ptr, False), "version": 2}
+
+    out = []
+    for ptr, rows, k in ((cx.edges, cx.n_edges, 2), (cx.tris, cx.n_tris, 3),
+                         (cx.tets, cx.n_tets, 4)):
+        if rows == 0:
+            out.append(np.zeros((0, k), np.uint32))
+            continue
+        addr = ctypes.cast(ptr, ctypes.c_void_p).value
+        t = torch.as_tensor(_View(addr, rows * k), device="cuda")
+        out.append(t.cpu().numpy().view(np.uint32).reshape(rows, k))
+    return out
 
 
 def main():
@@ -261,6 +254,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_BALLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-molecules", type=int, default=4096)
+    ap.add_argument("--no-exact", action="store_true",
+                    help="skip the decision-exact (precision cascade) measurements")
     ap.add_argument("--no-assembly", action="store_true",
                     help="skip the 2.5M-ball assembly pass reported beside the headline")
     args = ap.parse_args()
@@ -318,6 +313,18 @@ def main():
         barrier()
         wall = time.perf_counter() - t0
     step_ms = [a.elapsed_time(b) for a, b in ev]
+
+    # ---- parity of the last timed pass: its lists and stage counters
+    # against the restatement's digests (tests/golden/headline_100k.json),
+    # outside the timed region
+    parity = {}
+    head = _golden("headline_100k.json")
+    if head and rank == 0 and n == head["balls"]:
+        E, T, Q = _device_lists(cx)
+        s_last = stats[-1]
+        parity["headline_100k"] = ([_sha(E), _sha(T), _sha(Q)] == head["sha256"] and
+                                   all(s_last[k] == v for k, v in head["stats"].items()))
+        del E, T, Q
     dev_ms = sum(step_ms)
 
     # ---- union volume/area and their gradients on the final complex
@@ -429,6 +436,14 @@ def main():
                    np.array_equal(r.tris, b.tris) and np.array_equal(r.edges, b.edges)
                    for r, b in zip(plain, bres))
         del plain
+        bman = _golden("batch_4096.json")
+        if bman and len(sizes) == bman["molecules"]:
+            import hashlib
+            h = [hashlib.sha256() for _ in range(3)]
+            for r in bres:
+                for k, a in enumerate((r.edges, r.tris, r.tets)):
+                    h[k].update(np.ascontiguousarray(a, dtype=np.uint32).tobytes())
+            parity["batch_4096"] = [x.hexdigest() for x in h] == bman["sha256_concat"]
         batched = {"molecules": int(len(sizes)), "balls": int(boff[-1]), "sol_rad": SOL,
                    "alpha": 0.5, "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
                    "speedup": t_plain / t_batch, "identical_output": bool(same),
@@ -439,6 +454,49 @@ def main():
                                          "ms_tri_attach", "ms_edge_attach", "ms_emit", "ms_d2h")},
                    "what": "host C ABI both ways (wall clock): one pac_alpha_complex_batch "
                            "call vs one pac_alpha_complex call per molecule"}
+
+    # ---- the precision cascade (PAC_PRED_EXACT): every decision exact, an
+    # FP64 filter with a running error bound and 640-bit integers where it
+    # cannot tell; throughput on the headline workload and on the 25,000-ball
+    # lattice-snapped degeneracy case, with the fallback rates
+    exact = None
+    if not args.no_exact:
+        def timed(engine, dptr, count, sol, alpha, reps=3):
+            engine.alpha_complex_device(dptr, count, sol, alpha)  # sizes the pool
+            ms, st_ = [], None
+            for _ in range(reps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                st_ = engine.alpha_complex_device(dptr, count, sol, alpha)[1]
+                ms.append(st_["ms_total"])
+            return min(ms), st_
+
+        exact = {"what": "PAC_PRED_EXACT: FP64 filter with a running error bound, 640-bit "
+                         "integer fallback; fallback_rate = exact_fallbacks / filter_evals"}
+        with pac.Engine(device=local, tet_mode="as-written", predicates="exact") as ex:
+            ms, st_ = timed(ex, d_balls.data_ptr(), n, SOL, ALPHA)
+            exact["headline_100k"] = {
+                "ms": ms, "balls_per_s": n / (ms / 1e3), "filter_evals": st_["filter_evals"],
+                "exact_fallbacks": st_["exact_fallbacks"],
+                "fallback_rate": st_["exact_fallbacks"] / max(1, st_["filter_evals"]),
+                "complex": [st_["final_edges"], st_["final_tris"], st_["final_tets"]]}
+        snap = pac.snapped_globule(25_000, seed=pac.SEED_BASE + 1)
+        d_snap = torch.from_numpy(snap).cuda()
+        torch.cuda.synchronize()
+        rec = {"balls": len(snap), "sol_rad": SOL, "alpha": ALPHA,
+               "workload": "25,000-ball globule, centres snapped to 0.25 A, radii to 0.05 A"}
+        for mode in ("strict", "exact"):
+            with pac.Engine(device=local, tet_mode="as-written", predicates=mode) as ex:
+                ms, st_ = timed(ex, d_snap.data_ptr(), len(snap), SOL, ALPHA)
+            rec[mode] = {"ms": ms, "balls_per_s": len(snap) / (ms / 1e3),
+                         "sos_calls": st_["sos_calls"],
+                         "complex": [st_["final_edges"], st_["final_tris"], st_["final_tets"]]}
+            if mode == "exact":
+                rec[mode].update(filter_evals=st_["filter_evals"],
+                                 exact_fallbacks=st_["exact_fallbacks"],
+                                 fallback_rate=st_["exact_fallbacks"] / max(1, st_["filter_evals"]))
+        exact["snapped_25k"] = rec
+        del d_snap
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -459,7 +517,8 @@ def main():
         / (ms_per_step / 1e3),
         "complex": {"edges": s0["final_edges"], "tris": s0["final_tris"], "tets": s0["final_tets"],
                     "cand_tets": s0["cand_tets"], "alpha_tets": s0["alpha_tets"],
-                    "insphere_evals": s0["insphere_evals"], "sos_calls": s0["sos_calls"]},
+                    "insphere_evals": s0["insphere_evals"], "sos_calls": s0["sos_calls"],
+                    "early_refuted": s0["early_refuted"], "cert_decisions": s0["cert_decisions"]},
         "stage_ms": {k: s0[k] for k in ("ms_grid", "ms_edges", "ms_tris", "ms_tets",
                                         "ms_tri_attach", "ms_edge_attach", "ms_emit")},
         "union": {"grad_ms": grad_ms, "volume": uvol, "area": uarea,
@@ -471,7 +530,7 @@ def main():
                 "host_wall_ms_per_step": 1e3 * sum(e2e_wall) / len(e2e_wall)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "tetrahedron stage (k_tets_alpha1 + k_tets_alpha_rows + k_tets_scan + k_sos_resolve)",
+                     "kernel": "tetrahedron stage (k_tets_enum light + heavy, k_tets_scan, k_sos_resolve)",
                      "bytes_model": "64 B x candidate tetrahedra (the reference's tetrahedron "
                                     "and orthosphere lists written and read once)",
                      "kernel_ms": tet_ms},
@@ -482,6 +541,8 @@ def main():
                           "frac": s0["bytes_model"] / (ms_per_step / 1e3) / 1e9 / peak,
                           "bytes": s0["bytes_model"]},
         "cpu_baseline": cpu,
+        "parity": parity,
+        "exact": exact,
         "gpu_launches": int(sum(s["kernels_launched"] for s in stats)),
         "clocks": clocks,
         "wall_s": wall,

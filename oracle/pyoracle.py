@@ -129,6 +129,32 @@ def exact_pred(kind, balls, alpha=0.0):
                                 float(alpha))
 
 
+SEED_BASE = 0xA1FA0000
+
+
+def globule(n, seed=SEED_BASE):
+    """The seeded self-avoiding-walk globule (the workload generator,
+    compiled into this library too, so that the checker needs nothing of
+    the product's)."""
+    L = lib()
+    L.pac_synth_globule.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p]
+    out = np.zeros((n, 4), np.float32)
+    if L.pac_synth_globule(seed, n, out.ctypes.data) != 0:
+        raise MemoryError("generator allocation failed")
+    return out
+
+
+def pad_corners(balls, margin=12.0, radius=1.7):
+    """balls plus 8 isolated balls at the corners of their bounding box grown
+    by `margin` A (the bench's padding; see the package's pad_corners)."""
+    b = np.asarray(balls, dtype=np.float32)
+    lo = b[:, :3].min(0) - margin
+    hi = b[:, :3].max(0) + margin
+    corners = [[(lo, hi)[i][0], (lo, hi)[j][1], (lo, hi)[k][2], radius]
+               for i in (0, 1) for j in (0, 1) for k in (0, 1)]
+    return np.concatenate([b, np.array(corners, np.float32)])
+
+
 def canonical(a):
     """Sort vertices within each simplex, then the rows lexicographically."""
     a = np.sort(np.asarray(a, dtype=np.int64), axis=1)

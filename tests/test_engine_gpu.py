@@ -412,3 +412,25 @@ def test_batch_4096_matches_restatement_digests(pac):
             h[k].update(np.ascontiguousarray(a, dtype=np.uint32).tobytes())
     assert [x.hexdigest() for x in h] == man["sha256_concat"]
     print("batch of 4,096: %d simplices, %.0f ms" % (got.sum(), st["ms_total"]))
+
+
+@pytest.mark.parametrize("name", ["plain_1grm_a1", "plain_1k4c_a1", "plain_glob1300_a0",
+                                  "plain_glob5000_s14_a1", "plain_glob3000_s14_a05"])
+def test_engine_matches_plain_reference_binary(pac, name):
+    """Plain-xmp formulas (AlphaComplexParallel.cu:203-230, 310-372), as
+    written, strict flavour == the reference's plain binary built with
+    -maxrregcount=128 -fmad=false and run on a B200, list for list in the
+    binary's output order (fixtures by tests/golden/make_refrun_golden.py)."""
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "refrun", "refrun_manifest.json")))[name]
+    src = {"plain_1grm_a1": lambda: golden("1grm_ld_alpha1")[0],
+           "plain_1k4c_a1": lambda: golden("1k4c_plain_alpha1")[0],
+           "plain_glob1300_a0": lambda: pac.globule(1300, seed=pac.SEED_BASE),
+           "plain_glob5000_s14_a1": lambda: pac.pad_corners(pac.globule(5000, seed=pac.SEED_BASE + 4)),
+           "plain_glob3000_s14_a05": lambda: pac.pad_corners(pac.globule(3000, seed=pac.SEED_BASE + 7))}
+    balls = src[name]()
+    assert len(balls) == man["n"]
+    with _engine(pac, 1, "as-written", "strict") as eng:
+        r = eng.alpha_complex(balls, man["sol_rad"], man["alpha"])
+    _same(r, *_refrun(name, "plain-rr128-nofma"))
+

@@ -249,3 +249,23 @@ def test_default_reference_build_aborts_on_b200():
             continue
         assert e["builds"]["default"]["rc"] != 0
         assert "system_error" in e["builds"]["default"]["log_tail"]
+
+
+def test_headline_matches_reference_binary_record():
+    """The reference binary's own run on the headline workload (one B200 run
+    of the -fmad=false build, 254 s) produced the lists the headline digest
+    holds: the digest is the reference's, not only the restatement's."""
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "refrun", "refrun_manifest.json")))
+    head = json.load(open(os.path.join(GOLDEN, "headline_100k.json")))
+    rec = man["glob100k_s14_a1"]["builds"]["rr128-nofma"]
+    assert rec["rc"] == 0 and rec["sha256"] == head["sha256"] and rec["counts"] == head["counts"]
+
+
+def test_oracle_generator_equals_package_generator(pac, orc):
+    """The oracle library carries its own copy of the workload generator
+    (so the bench's reference arm loads nothing of the product); both give
+    the same balls."""
+    a = pac.pad_corners(pac.globule(3000, seed=pac.SEED_BASE + 4))
+    b = orc.pad_corners(orc.globule(3000, seed=orc.SEED_BASE + 4))
+    assert np.array_equal(a, b)
