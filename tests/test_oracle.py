@@ -244,11 +244,11 @@ def test_default_reference_build_aborts_on_b200():
     """Built with default flags, the reference aborts on a B200 once
     checkTetsOrthosphere fails to launch; recorded, not re-run."""
     man = _refrun_manifest()
-    for name, e in man.items():
-        if "skipped" in e:
-            continue
-        assert e["builds"]["default"]["rc"] != 0
-        assert "system_error" in e["builds"]["default"]["log_tail"]
+    runs = [e["builds"]["default"] for e in man.values() if "default" in e.get("builds", {})]
+    assert runs
+    for rec in runs:
+        assert rec["rc"] != 0
+        assert "system_error" in rec["log_tail"]
 
 
 def test_headline_matches_reference_binary_record():
