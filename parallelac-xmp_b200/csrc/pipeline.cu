@@ -1174,14 +1174,11 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
     for (int k0 = 0; k0 < nb; k0 += 32) {
         const int nj = min(32, nb - k0);
         // lane j: the fourth vertices c > b with the three faces at p
-        // (ra & L[b] & above b) whose face (v2, v3, v4) is in v2's link
+        // (ra & L[b] & above b)
         uint64_t pm[KW];
-        int mb = 0xffff;
-        const uint64_t *R2 = sL2;
         if (lane < nj) {
             const int b = sBl[k0 + lane];
-            mb = smap[b];
-            R2 = l2s ? sL2 + mb * W2 : L2g + (uint64_t)mb * W2;
+            const int mb = smap[b];  // 0xffff: (v2, v3) has no alpha edge in v2's list
 #pragma unroll
             for (int w = 0; w < KW; w++)
                 pm[w] = (w < W && mb != 0xffff) ? (ra[w] & L[(uint64_t)b * W + w] & above_mask(b, w))
@@ -1190,26 +1187,17 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
 #pragma unroll
             for (int w = 0; w < KW; w++) pm[w] = 0ull;
         }
-        // count pass (face check per bit), then write pass below
+        // the pre-candidates (faces at p only); the face (v2, v3, v4) is
+        // checked in the batches below, where every lane is busy
         int cnt = 0;
 #pragma unroll
-        for (int w = 0; w < KW; w++) {
-            uint64_t bits = pm[w];
-            while (bits) {
-                const int c = w * 64 + __ffsll((long long)bits) - 1;
-                bits &= bits - 1;
-                const int mc = smap[c];
-                if (mc != 0xffff && ((R2[mc >> 6] >> (mc & 63)) & 1ull)) cnt++;
-                else pm[w] &= ~(1ull << (c & 63));
-            }
-        }
+        for (int w = 0; w < KW; w++) cnt += __popcll(pm[w]);
         int incl = cnt;
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(kFull, incl, o);
             if (lane >= o) incl += v;
         }
         const int total = __shfl_sync(kFull, incl, 31);
-        if (lane == 0) cand_acc += total;
         // best-so-far slots of the chunk's groups (j, side)
         S.best[wib][lane] = ~0ull;
         S.best[wib][lane + 32] = ~0ull;
@@ -1242,11 +1230,21 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
                     c = (int)(e >> 8);
                 }
                 const int b = act ? (int)sBl[k0 + j] : 0;
+                bool face = false;
+                if (act) {  // (v2, v3, v4) an alpha triangle: bit of v2's link
+                    const int mb = smap[b], mc = smap[c];
+                    if (mc != 0xffff) {
+                        const uint64_t at2 = (uint64_t)mb * W2 + (mc >> 6);
+                        face = ((l2s ? sL2[at2] : __ldg(&L2g[at2])) >> (mc & 63)) & 1ull;
+                    }
+                }
+                const unsigned mF = __ballot_sync(kFull, face);
+                if (lane == 0) cand_acc += __popc(mF);
                 bool passA = false, side = false;
                 float4 sphere = make_float4(0.f, 0.f, 0.f, 0.f);
                 float key = 0.f;
                 Ball B3{0.f, 0.f, 0.f, 0.f}, B4{0.f, 0.f, 0.f, 0.f};
-                if (act) {
+                if (face) {
                     const float4 b3 = sb[b], b4 = sb[c];
                     B3 = Ball{b3.x, b3.y, b3.z, b3.w};
                     B4 = Ball{b4.x, b4.y, b4.z, b4.w};
@@ -1360,6 +1358,7 @@ __global__ void __launch_bounds__(EnumSmem<KW>::kWarps * 32, KW == 1 ? 3 : 4)
             const uint32_t x = __ldg(&Ng[c]);
             S.sN[wib][c] = x;
             S.sb[wib][c] = __ldg(&A.at[x]);
+
             if constexpr (KW == 1) S.sL[wib][c] = Lg[c];
         }
         const Ball B1 = pac::ld_ball(&A.at[p]);
