@@ -190,6 +190,10 @@ typedef struct {
        verify mode the certified decisions the replay disagrees with */
     uint64_t early_refuted, early_tests;
     uint64_t cert_decisions, cert_disagreements;
+    /* the part of ms_tets spent in the empty-orthosphere test (the scan and
+       the simulation-of-simplicity kernel): the reference's "AC2 test for
+       tetrahedra" phase (AlphaComplexLargeData.cu:2014) */
+    double ms_tet_orthosphere;
 } pac_stats;
 
 /* Version of this ABI (PAC_ABI_VERSION). */

@@ -75,7 +75,8 @@ class Stats(ctypes.Structure):
                 [(k, ctypes.c_double) for k in _STAT_F64] +
                 [("bytes_model", ctypes.c_uint64), ("grid", ctypes.c_uint32 * 3),
                  ("step", ctypes.c_float), ("kernels_launched", ctypes.c_uint32)] +
-                [(k, ctypes.c_uint64) for k in _STAT_U64B])
+                [(k, ctypes.c_uint64) for k in _STAT_U64B] +
+                [("ms_tet_orthosphere", ctypes.c_double)])
 
     def as_dict(self):
         d = {k: int(getattr(self, k)) for k in _STAT_U64}
@@ -85,6 +86,7 @@ class Stats(ctypes.Structure):
         d["step"] = float(self.step)
         d["kernels_launched"] = int(self.kernels_launched)
         d.update({k: int(getattr(self, k)) for k in _STAT_U64B})
+        d["ms_tet_orthosphere"] = float(self.ms_tet_orthosphere)
         return d
 
 

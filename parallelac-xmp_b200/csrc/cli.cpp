@@ -43,8 +43,16 @@ int main(int argc, char **argv) {
         "alpha = %.3f and solvent radius = %.3f ...\n\n",
         (int)n, alpha, solventRadius);
 #ifdef PAC_CLI_LARGEDATA
-    std::printf("Processed %d atoms ... \n", 0);
-    (void)std::atoi(argv[5]);
+    // the reference's chunk (512 doubled up to the suggestion) and its
+    // per-chunk progress line (AlphaComplexLargeData.cu:1227-1235); the pass
+    // itself is one device pass whatever the chunk
+    {
+        const int suggestion = std::atoi(argv[5]);
+        long long chunk = 512;
+        while (chunk < suggestion) chunk *= 2;
+        for (long long start = 0; start < (long long)n; start += chunk)
+            std::printf("Processed %lld atoms ... \n", start);
+    }
 #endif
     pac_options opt;
     pac_default_options(&opt);
@@ -80,8 +88,9 @@ int main(int argc, char **argv) {
         "\nTime taken (ms):\nData transfer: %20.3f\nGrid computation: %17.3f\nPotential edges: %18.3f\n"
         "Potential triangles: %14.3f\nPotential tetrahedra: %13.3f\nAC2 test for tetrahedra: %10.3f\n"
         "AC2 test for triangles: %11.3f\nAC2 test for edges: %15.3f\n",
-        st.ms_h2d + st.ms_d2h + st.ms_emit, st.ms_grid, st.ms_edges, st.ms_tris, st.ms_tets, 0.0,
-        st.ms_tri_attach, st.ms_edge_attach);
+        st.ms_h2d + st.ms_d2h + st.ms_emit, st.ms_grid, st.ms_edges, st.ms_tris,
+        st.ms_tets - st.ms_tet_orthosphere, st.ms_tet_orthosphere, st.ms_tri_attach,
+        st.ms_edge_attach);
     std::printf("Total time taken (ms): %12.3f\n", st.ms_total);
     std::printf("\nWriting computed alpha complex to the file %s ...\n", argv[2]);
     rc = pac_write_complex(argv[2], balls, n, solventRadius, &cx);

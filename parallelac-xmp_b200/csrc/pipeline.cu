@@ -1424,7 +1424,7 @@ constexpr int kScanStep = 4;
 // arithmetic; A.verify replays every certified decision too and counts
 // disagreements (C_CERT_BAD).  Survivors are recorded and mark their faces.
 template <int V>
-__global__ void __launch_bounds__(256, 3) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
+__global__ void __launch_bounds__(256, 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
@@ -2015,8 +2015,8 @@ struct Timer {
     pac::Ctx &ctx;
     int i = 0;
     explicit Timer(pac::Ctx &c) : ctx(c) {}
-    void mark() {
-        if (i < 16) cudaEventRecord(ctx.ev[i++], ctx.stream);
+    void mark() {  // events 0..13 (14 and 15 time the orthosphere test)
+        if (i < 14) cudaEventRecord(ctx.ev[i++], ctx.stream);
     }
     double ms(int a, int b) {
         float f = 0;
@@ -2232,6 +2232,16 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         }
         rc = enum_smem_optin<V>(ctx);
         if (rc) return rc;
+        // the empty-orthosphere test's share of the stage: ev[14], ev[15]
+        // around each scan, read once the stream has passed them
+        double ortho_ms = 0.0;
+        bool ortho_pending = false;
+        auto ortho_collect = [&]() {
+            if (!ortho_pending) return;
+            float f = 0.f;
+            if (cudaEventElapsedTime(&f, ctx.ev[14], ctx.ev[15]) == cudaSuccess) ortho_ms += f;
+            ortho_pending = false;
+        };
         unsigned long long cand_total = 0, alpha_total = 0;
         uint64_t lo = 0, chunk = n;
         // verbose: per-chunk enumeration and scan times
@@ -2261,6 +2271,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             CK(cudaMemcpyAsync(ha, ctrA, sizeof(ha), cudaMemcpyDeviceToHost, s));
             CK(cudaMemcpyAsync(used, ctr + C_SURV, sizeof(used), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
+            ortho_collect();
             const unsigned long long queued = ha[C_SURV];
             if (queued > qcap) {
                 if (hi - lo == 1)
@@ -2299,8 +2310,11 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             }
             CK(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
             if (queued) {
+                CK(cudaEventRecord(ctx.ev[14], s));
                 k_tets_scan<V><<<148 * std::max(1, cfg.scan_blocks), 256, 0, s>>>(T, Q, queued, claim);
                 LAUNCH_CHECK(ctx);
+                CK(cudaEventRecord(ctx.ev[15], s));
+                ortho_pending = true;
             }
             if (cfg.verbose) {
                 float me = 0.f, ms = 0.f;
@@ -2331,6 +2345,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         unsigned long long sp[2];
         CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(sp), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        ortho_collect();
         if (sp[0] > T.surv_cap || sp[1] > T.pend_cap)
             return pac::set_error(PAC_ERR_CAPACITY, "tetrahedron survivor buffer overflow");
         if (sp[1] && sp[0] + sp[1] > T.surv_cap) {  // resolved entries join the survivors
@@ -2342,11 +2357,16 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             T.surv_cap = sp[0] + sp[1];
         }
         if (sp[1]) {
+            CK(cudaEventRecord(ctx.ev[14], s));
             k_sos_resolve<V><<<blocks_for(sp[1], 64), 64, 0, s>>>(T, sp[1]);
             LAUNCH_CHECK(ctx);
+            CK(cudaEventRecord(ctx.ev[15], s));
+            ortho_pending = true;
             CK(cudaMemcpyAsync(sp, ctr + C_SURV, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
+            ortho_collect();
         }
+        if (st) st->ms_tet_orthosphere = ortho_ms;
         nQ = sp[0];
         rc = exclusive_scan(ctx, T.tcount, n, toff);
         if (rc) return rc;

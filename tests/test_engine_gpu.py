@@ -199,6 +199,29 @@ def test_device_entry_point(pac):
 
 
 # ------------------------------------------------------------ CLI
+def test_cli_report_phases_and_progress(pac, tmp_path):
+    """The CLI's report follows the reference's: one "Processed N atoms"
+    line per reference chunk (512 doubled up to the suggestion,
+    AlphaComplexLargeData.cu:1227-1235) and, as written, the
+    empty-orthosphere test reported as its own phase ("AC2 test for
+    tetrahedra", AlphaComplexLargeData.cu:2014)."""
+    balls = pac.globule(3000, seed=pac.SEED_BASE + 5)
+    crd = tmp_path / "g.crd"
+    with open(crd, "w") as f:
+        f.write("%d\n" % len(balls))
+        for b in balls:
+            f.write("%s %s %s %s\n" % tuple(repr(float(v)) for v in b))
+    exe = os.path.join(pac.BIN_DIR, "parallelac-largeData")
+    r = subprocess.run([exe, str(crd), str(tmp_path / "o.txt"), "1.4", "1", "1000"],
+                       capture_output=True, text=True,
+                       env=dict(os.environ, PAC_TET_MODE="as-written"))
+    assert r.returncode == 0, r.stderr
+    starts = [int(l.split()[1]) for l in r.stdout.splitlines() if l.startswith("Processed")]
+    assert starts == [0, 1024, 2048]
+    ac2 = [l for l in r.stdout.splitlines() if l.startswith("AC2 test for tetrahedra:")]
+    assert len(ac2) == 1 and float(ac2[0].split(":")[1]) > 0.0
+
+
 def test_cli_reproduces_golden_file(pac, tmp_path):
     import gzip
     balls, _, _, _ = golden("1grm_ld_alpha1")
@@ -335,7 +358,7 @@ def test_autotuner_passes_all_give_the_same_lists(pac, orc):
     balls = pac.globule(3000, seed=pac.SEED_BASE + 81)
     e, t, q, _ = orc.alpha_complex(balls, 1.4, 1.0, orc.UPSTREAM, tet_ortho=True)
     with pac.Engine(autotune=True) as eng:
-        for _ in range(10):  # 8 candidate shapes, then the chosen one
+        for _ in range(14):  # 12 candidate shapes, then the chosen one
             _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
     with pac.Engine(enum_blocks=2, scan_blocks=2, heavy_blocks=3, unit_rows=3, scan_claim=64) as eng:
         _same(eng.alpha_complex(balls, 1.4, 1.0), e, t, q)
