@@ -125,7 +125,15 @@ typedef struct {
        alpha tetrahedron goes to the scan; same lists).
        reserved_i[6] = 1: verify mode -- the scan also replays the
        reference's arithmetic for every decision the certified filter takes
-       and counts disagreements (pac_stats.cert_disagreements; 0 expected). */
+       and counts disagreements (pac_stats.cert_disagreements; 0 expected).
+       reserved_i[7] = W > 1, reserved_i[8] = r: slab r of W of one molecule
+       (as written only): the pass outputs the simplices whose smallest
+       vertex in cell order lies in the r-th of W contiguous ranges of the
+       cell-sorted balls (cut at cell starts), in the reference's order, so
+       that the W outputs concatenated in rank order are the whole complex.
+       Every rank holds all balls and computes the tetrahedron and triangle
+       stages from two cell layers below its range; no data is exchanged.
+       The stage counters then count the slab's work, halo included. */
     int reserved_i[9];
     /* reserved_u[0]: if nonzero, the number of alpha tetrahedra the pass
        queues per chunk (default: a quarter of free device memory, at most

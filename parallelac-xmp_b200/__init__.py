@@ -177,7 +177,7 @@ class Engine:
     def __init__(self, device=0, formula="upstream", tet_mode="as-written", predicates="strict",
                  order="reference", verbose=False, queue_entries=None, autotune=False,
                  enum_blocks=None, scan_blocks=None, heavy_blocks=None, unit_rows=None,
-                 scan_claim=None, refute=True, verify=False):
+                 scan_claim=None, refute=True, verify=False, slab=None):
         L = _lib()
         if L.pac_abi_version() != 2:
             raise RuntimeError("libpac.so ABI %d, this binding expects 2" % L.pac_abi_version())
@@ -198,6 +198,8 @@ class Engine:
                 o.reserved_i[k] = int(v)
         o.reserved_i[5] = 0 if refute else 1
         o.reserved_i[6] = 1 if verify else 0
+        if slab:  # (rank, world): one slab of a molecule partitioned by cell order
+            o.reserved_i[8], o.reserved_i[7] = int(slab[0]), int(slab[1])
         self._ctx = ctypes.c_void_p()
         _check(L.pac_create(ctypes.byref(self._ctx), ctypes.byref(o)))
 
@@ -452,14 +454,44 @@ def shard_molecules(sizes, world):
     return [np.array(sorted(p), dtype=np.int64) for p in parts]
 
 
+def _gather_rows(arrays, rank, world, group=None):
+    """Rank 0 receives every rank's 2-D uint32 arrays (one list of them per
+    rank, in rank order; None elsewhere): the row counts first (one
+    all_gather), then each array padded to the largest count (one gather
+    each) -- tensors, so NCCL or gloo moves them without pickling."""
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    counts = torch.tensor([len(a) for a in arrays], dtype=torch.int64, device=dev)
+    allc = [torch.zeros_like(counts) for _ in range(world)]
+    dist.all_gather(allc, counts, group=group)
+    allc = torch.stack(allc).cpu().numpy()
+    out = [[] for _ in range(world)] if rank == 0 else None
+    for k, a in enumerate(arrays):
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        width = a.shape[1]
+        rows = int(allc[:, k].max())
+        buf = torch.zeros((max(rows, 1), width), dtype=torch.int32, device=dev)
+        if len(a):
+            buf[:len(a)] = torch.from_numpy(a.view(np.int32)).to(dev)
+        recv = [torch.zeros_like(buf) for _ in range(world)] if rank == 0 else None
+        dist.gather(buf, recv, dst=0, group=group)
+        if rank == 0:
+            for r in range(world):
+                out[r].append(recv[r][:int(allc[r, k])].cpu().numpy().view(np.uint32))
+    return out
+
+
 def sharded_batch(balls, offsets, rank, world, run, group=None):
     """Many molecules over the ranks of a torch.distributed group: rank r
     computes the molecules shard_molecules() gives it with
     run(balls, offsets) -> [(edges, tris, tets)] (one rank-local batched
     pass, e.g. an Engine's alpha_complex_batch), and rank 0 receives every
     molecule's lists in the original order (None on the other ranks).  The
-    molecules are independent: the only collective is this final gather."""
-    import torch.distributed as dist
+    molecules are independent: the only collective is the final gather, of
+    tensors (each rank's lists concatenated, and per molecule its id and
+    row counts)."""
     off = np.asarray(offsets, dtype=np.uint64)
     sizes = np.diff(off.astype(np.int64))
     mine = shard_molecules(sizes, world)[rank]
@@ -469,13 +501,62 @@ def sharded_batch(balls, offsets, rank, world, run, group=None):
         res = run(np.concatenate(parts), loff)
     else:
         res = []
-    local = [(int(m), tuple(np.asarray(x) for x in r)) for m, r in zip(mine, res)]
-    gathered = [None] * world if rank == 0 else None
-    dist.gather_object(local, gathered, dst=0, group=group)
+    cat = [np.concatenate([np.asarray(r[k], np.uint32).reshape(-1, w) for r in res])
+           if len(res) else np.zeros((0, w), np.uint32) for k, w in enumerate((2, 3, 4))]
+    meta = np.array([[m] + [len(r[k]) for k in range(3)] for m, r in zip(mine, res)],
+                    np.uint32).reshape(-1, 4)
+    got = _gather_rows(cat + [meta], rank, world, group)
     if rank != 0:
         return None
     out = [None] * len(sizes)
-    for part in gathered:
-        for m, r in part:
-            out[m] = r
+    for r in range(world):
+        E, T, Q, M = got[r]
+        at = [0, 0, 0]
+        for m, ne, nt, nq in M:
+            cnt = (int(ne), int(nt), int(nq))
+            out[int(m)] = tuple(x[at[k]:at[k] + cnt[k]] for k, x in enumerate((E, T, Q)))
+            at = [at[k] + cnt[k] for k in range(3)]
     return out
+
+
+def slab_cuts(balls, sol_rad, alpha, world):
+    """The partition of one molecule that Engine(slab=(r, world)) uses, on
+    the host: the cell-sorted order of the balls (the reference's stable
+    sort by cell key, AlphaComplexLargeData.cu:65-78, 1174-1177; binary32
+    arithmetic as there) and the cuts [own_lo, own_hi) of each rank -- ball
+    positions n r / world rounded down to the start of their cell.  Returns
+    (order, cuts): order[k] is the input index of the k-th ball in cell
+    order, cuts has world + 1 entries."""
+    b = np.asarray(balls, dtype=np.float32)
+    n = len(b)
+    with np.errstate(all="ignore"):
+        lo = b[:, :3].min(0)
+        mr = b[:, 3].max()
+        step = np.float32(2.0) * np.sqrt(np.float32(mr * mr + np.float32(alpha)), dtype=np.float32)
+        ext = b[:, :3].max(0) - lo
+        g = (ext / step).astype(np.int64) + 1
+        c = ((b[:, :3] - lo) / step).astype(np.int64)
+    key = c[:, 0] + g[0] * c[:, 1] + g[0] * g[1] * c[:, 2]
+    order = np.argsort(key, kind="stable")
+    skey = key[order]
+    cuts = [0]
+    for r in range(1, world):
+        t = n * r // world
+        cuts.append(int(np.searchsorted(skey, skey[t], side="left")) if t < n else n)
+    cuts.append(n)
+    for r in range(1, world + 1):  # ranges stay ordered when cells are large
+        cuts[r] = max(cuts[r], cuts[r - 1])
+    return order, np.array(cuts, dtype=np.int64)
+
+
+def sharded_slab(balls, sol_rad, alpha, rank, world, engine, group=None):
+    """One molecule over the ranks of a torch.distributed group: rank r runs
+    engine.alpha_complex on its slab (the engine must be made with
+    slab=(rank, world)); rank 0 receives the whole complex, the ranks' lists
+    concatenated in rank order (None on the other ranks).  Every rank holds
+    all the balls; the only collective is the final gather."""
+    r = engine.alpha_complex(balls, sol_rad, alpha)
+    got = _gather_rows([r.edges, r.tris, r.tets], rank, world, group)
+    if rank != 0:
+        return None
+    return tuple(np.concatenate([got[q][k] for q in range(world)]) for k in range(3))

@@ -163,6 +163,8 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
     cfg.queue_entries = qbytes / 32;
     cfg.exact = c.opt.predicates == PAC_PRED_EXACT;
     cfg.refute = c.opt.reserved_i[5] != 1;
+    cfg.slab_world = c.opt.reserved_i[7] > 1 ? c.opt.reserved_i[7] : 1;
+    cfg.slab_rank = c.opt.reserved_i[8];
     cfg.verify = c.opt.reserved_i[6] == 1;
     cfg.enum_blocks = c.opt.reserved_i[0] > 0 ? c.opt.reserved_i[0] : shape->enum_blocks;
     cfg.scan_blocks = c.opt.reserved_i[1] > 0 ? c.opt.reserved_i[1] : shape->scan_blocks;
@@ -439,6 +441,8 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
     std::memset(out, 0, sizeof(*out));
     if (st) std::memset(st, 0, sizeof(*st));
     if (offsets[0] != 0) return pac::set_error(PAC_ERR_INVALID_ARG, "offsets[0] must be 0");
+    if (ctx->c.opt.reserved_i[7] > 1)
+        return pac::set_error(PAC_ERR_INVALID_ARG, "slab passes take one molecule");
     for (uint32_t m = 0; m < n_mol; m++)
         if (offsets[m + 1] < offsets[m])
             return pac::set_error(PAC_ERR_INVALID_ARG, "offsets must be non-decreasing");

@@ -61,6 +61,7 @@ struct PipelineConfig {
     int verbose;
     uint64_t queue_entries;  // alpha tetrahedra queued per chunk (32 B each)
     bool exact;              // decision-exact predicates (strict flavour only)
+    int slab_rank, slab_world;  // one slab of a partition by cell order (world > 1)
     bool refute;             // early refutation in the tetrahedron enumeration
     bool verify;             // replay every certified insphere decision (debug)
     // launch shapes (the output does not depend on them)

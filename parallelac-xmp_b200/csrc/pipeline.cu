@@ -1640,10 +1640,11 @@ __global__ void k_sos_resolve(TetArgs A, uint64_t npend) {
 // Survivors to per-ball rows: scatter, then order each ball's rows by
 // (a, b, c) -- the order in which the reference enumerates them.
 __global__ void k_tet_scatter(const uint2 *surv, uint64_t ns, const uint64_t *toff,
-                              uint32_t *cursor, uint32_t *keys) {
+                              uint32_t *cursor, uint32_t *keys, uint64_t p_lo, uint64_t p_hi) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ns) return;
     uint2 s = surv[t];
+    if (s.x < p_lo || s.x >= p_hi) return;  // a slab's halo: not this pass's output
     keys[toff[s.x] + atomicAdd(&cursor[s.x], 1u)] = s.y;
 }
 __global__ void k_tet_sort_emit(uint64_t n, const uint64_t *toff, uint32_t *keys,
@@ -1695,7 +1696,8 @@ __global__ void k_map4(uint64_t nq, const uint32_t *orig, uint32_t *tets) {
 constexpr int kTQCap = 256;
 
 template <int V>
-__global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t n, const float4 *__restrict__ at,
+__global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t p_lo, uint64_t n,
+                                                       const float4 *__restrict__ at,
                                                        const uint64_t *__restrict__ eoff,
                                                        const uint32_t *__restrict__ ER,
                                                        const uint64_t *__restrict__ loff,
@@ -1711,7 +1713,7 @@ __global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t n, const float4 
     Tally tally;
     while (true) {
         uint64_t p = 0;
-        if (lane == 0) p = atomicAdd(&ctr[C_NEXT], 1ull);
+        if (lane == 0) p = p_lo + atomicAdd(&ctr[C_NEXT], 1ull);
         p = __shfl_sync(kFull, p, 0);
         if (p >= n) break;
         const uint64_t e0 = eoff[p];
@@ -1869,7 +1871,8 @@ __global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t n, const float4 
 // Final edges: edges of final triangles, plus the alpha edges whose radical
 // foot no other ball reaches (checkDanglingEdges, AlphaComplexLargeData.cu:924-1011).
 template <int V>
-__global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__restrict__ at,
+__global__ void __launch_bounds__(256) k_edge_final(uint64_t p_lo, uint64_t n,
+                                                    const float4 *__restrict__ at,
                                                     const uint64_t *__restrict__ eoff,
                                                     const uint32_t *__restrict__ ER,
                                                     uint8_t *eflag, const uint32_t *cellbeg,
@@ -1880,7 +1883,7 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t n, const float4 *__
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long oob = 0;
     Tally tally;
-    for (uint64_t p = warp; p < n; p += nwarps) {
+    for (uint64_t p = p_lo + warp; p < n; p += nwarps) {
         const uint64_t e0 = eoff[p];
         const int deg = (int)(eoff[p + 1] - e0);
         if (!deg) continue;
@@ -1949,14 +1952,14 @@ __global__ void k_emit_edges(uint64_t n, const uint64_t *eoff, const uint32_t *E
             out[2 * q + 1] = orig[ER[k]];
         }
 }
-__global__ void __launch_bounds__(256) k_emit_tris(uint64_t n, const uint64_t *eoff,
+__global__ void __launch_bounds__(256) k_emit_tris(uint64_t p_lo, uint64_t n, const uint64_t *eoff,
                                                    const uint32_t *ER, const uint64_t *loff,
                                                    const uint64_t *faces, const uint64_t *tpos,
                                                    const uint32_t *orig, uint32_t *out) {
     const int lane = threadIdx.x & 31;
     uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t p = warp; p < n; p += nwarps) {
+    for (uint64_t p = p_lo + warp; p < n; p += nwarps) {
         const int deg = (int)(eoff[p + 1] - eoff[p]);
         if (deg < 2) continue;
         const int W = (deg + 63) >> 6;
@@ -2115,6 +2118,51 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     LAUNCH_CHECK(ctx);
     tm.mark();  // 1
 
+    // ---- a slab of one molecule (cfg.slab_world > 1): this pass emits the
+    // simplices whose smallest vertex in cell order lies in [own_lo, own_hi)
+    // -- balls n r / world .. n (r + 1) / world rounded down to cell starts --
+    // and computes the tetrahedron and triangle stages from work_lo, two cell
+    // layers lower: every vertex of an alpha simplex lies in a cell adjacent
+    // to its smallest vertex's (alpha edges join adjacent cells), so the
+    // tetrahedra whose faces decide the owned triangles, and the triangles
+    // whose edges decide the owned edges, all start at or above work_lo.
+    uint64_t own_lo = 0, own_hi = n, work_lo = 0;
+    if (cfg.slab_world > 1) {
+        if (nm != 1)
+            return pac::set_error(PAC_ERR_INVALID_ARG, "a slab pass takes one molecule");
+        if (cfg.tet_mode != PAC_TETS_AS_WRITTEN)
+            return pac::set_error(PAC_ERR_INVALID_ARG, "a slab pass applies the orthosphere test");
+        if (cfg.slab_rank < 0 || cfg.slab_rank >= cfg.slab_world)
+            return pac::set_error(PAC_ERR_INVALID_ARG, "slab rank out of range");
+        auto cell_start = [&](uint64_t ball, uint64_t &out) -> int {
+            if (ball >= n) {
+                out = n;
+                return PAC_OK;
+            }
+            uint32_t c = 0, b = 0;
+            CK(cudaMemcpyAsync(&c, cellof + ball, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            CK(cudaMemcpyAsync(&b, cellbeg + c, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            out = b;
+            return PAC_OK;
+        };
+        const uint64_t r = (uint64_t)cfg.slab_rank, w = (uint64_t)cfg.slab_world;
+        if (r > 0 && (rc = cell_start(n * r / w, own_lo))) return rc;
+        if (r + 1 < w && (rc = cell_start(n * (r + 1) / w, own_hi))) return rc;
+        if (own_hi < own_lo) own_hi = own_lo;
+        if (own_lo > 0) {
+            uint32_t c = 0, b = 0;
+            CK(cudaMemcpyAsync(&c, cellof + own_lo, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            const uint64_t layer = (uint64_t)hg[0].gx * hg[0].gy + hg[0].gx + 1;
+            const uint64_t c0 = c > 2 * layer ? c - 2 * layer : 0;
+            CK(cudaMemcpyAsync(&b, cellbeg + c0, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            work_lo = b;
+        }
+    }
+
     // ---- alpha edges
     uint32_t *ecount = ar.alloc_n<uint32_t>(n);
     uint64_t *eoff = ar.alloc_n<uint64_t>(n + 1);
@@ -2181,7 +2229,8 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     T.tcount = ar.alloc_n<uint32_t>(n);
     uint64_t *toff = ar.alloc_n<uint64_t>(n + 1);
     if (!T.tcount || !toff) return PAC_ERR_OOM;
-    uint64_t nQ = 0;
+    uint64_t nQ = 0;      // tetrahedra output
+    uint64_t nQ_all = 0;  // survivors, a slab's halo included
     uint32_t *tets_sorted = nullptr;
     if (cfg.tet_mode == PAC_TETS_AS_RUN) {
         k_tets<V, 1><<<warp_blocks(n), 256, 0, s>>>(T);
@@ -2243,15 +2292,15 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             ortho_pending = false;
         };
         unsigned long long cand_total = 0, alpha_total = 0;
-        uint64_t lo = 0, chunk = n;
+        uint64_t lo = work_lo, chunk = n;
         // verbose: per-chunk enumeration and scan times
         cudaEvent_t vev[3] = {nullptr, nullptr, nullptr};
         if (cfg.verbose)
             for (auto &e : vev) CK(cudaEventCreate(&e));
         const unsigned enum_blocks = 148u * (unsigned)std::max(1, cfg.enum_blocks);
         const unsigned heavy_blocks = 148u * (unsigned)std::max(1, cfg.heavy_blocks);
-        while (lo < n) {
-            const uint64_t hi = std::min<uint64_t>(n, lo + chunk);
+        while (lo < own_hi) {
+            const uint64_t hi = std::min<uint64_t>(own_hi, lo + chunk);
             TetArgs TA = T;
             TA.ctr = ctrA;
             if (cfg.verbose) CK(cudaEventRecord(vev[0], s));
@@ -2368,8 +2417,15 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         }
         if (st) st->ms_tet_orthosphere = ortho_ms;
         nQ = sp[0];
+        if (cfg.slab_world > 1 && own_lo > 0)  // the halo's tetrahedra are not output
+            CK(cudaMemsetAsync(T.tcount, 0, sizeof(uint32_t) * own_lo, s));
         rc = exclusive_scan(ctx, T.tcount, n, toff);
         if (rc) return rc;
+        if (cfg.slab_world > 1) {
+            nQ_all = nQ;
+            CK(cudaMemcpyAsync(&nQ, toff + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
     }
     tm.mark();  // 4
 
@@ -2379,13 +2435,26 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
     if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
     CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
-    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(n), 148 * 4), 256, 0, s>>>(
-        n, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids, in.alpha, ctr);
+    if (cfg.slab_world > 1) CK(cudaMemsetAsync(tricount, 0, sizeof(uint32_t) * n, s));
+    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(own_hi - work_lo), 148 * 4), 256, 0, s>>>(
+        work_lo, own_hi, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids,
+        in.alpha, ctr);
     LAUNCH_CHECK(ctx);
     tm.mark();  // 5
-    k_edge_final<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, eflag, cellbeg, mol, grids,
-                                                   ctr);
+    k_edge_final<V><<<warp_blocks(own_hi - own_lo), 256, 0, s>>>(own_lo, own_hi, at, eoff, ER, eflag,
+                                                                 cellbeg, mol, grids, ctr);
     LAUNCH_CHECK(ctx);
+    if (cfg.slab_world > 1) {
+        // only the owned balls' triangles and edges are output
+        if (own_lo > work_lo)
+            CK(cudaMemsetAsync(tricount + work_lo, 0, sizeof(uint32_t) * (own_lo - work_lo), s));
+        uint64_t eb[2] = {0, 0};
+        CK(cudaMemcpyAsync(&eb[0], eoff + own_lo, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&eb[1], eoff + own_hi, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (eb[0]) CK(cudaMemsetAsync(eflag, 0, eb[0], s));
+        if (nE > eb[1]) CK(cudaMemsetAsync(eflag + eb[1], 0, nE - eb[1], s));
+    }
     tm.mark();  // 6
 
     // ---- emission
@@ -2403,7 +2472,8 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     if (!out.d_edges || !out.d_tris || !out.d_tets) return PAC_ERR_OOM;
     k_emit_edges<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, ER, eflag, epos, orig, out.d_edges);
     LAUNCH_CHECK(ctx);
-    k_emit_tris<<<warp_blocks(n), 256, 0, s>>>(n, eoff, ER, loff, faces, tpos, orig, out.d_tris);
+    k_emit_tris<<<warp_blocks(own_hi - own_lo), 256, 0, s>>>(own_lo, own_hi, eoff, ER, loff, faces,
+                                                            tpos, orig, out.d_tris);
     LAUNCH_CHECK(ctx);
     if (cfg.tet_mode == PAC_TETS_AS_RUN) {
         CK(cudaMemcpyAsync(out.d_tets, tets_sorted, sizeof(uint32_t) * 4 * (nQ ? nQ : 1),
@@ -2414,7 +2484,9 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         uint32_t *cursor = ar.alloc_n<uint32_t>(n), *keys = ar.alloc_n<uint32_t>(nQ);
         if (!cursor || !keys) return PAC_ERR_OOM;
         CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * n, s));
-        k_tet_scatter<<<blocks_for(nQ, 256), 256, 0, s>>>(T.surv, nQ, toff, cursor, keys);
+        const uint64_t ns = std::max(nQ, nQ_all);
+        k_tet_scatter<<<blocks_for(ns, 256), 256, 0, s>>>(T.surv, ns, toff, cursor, keys, own_lo,
+                                                          own_hi);
         LAUNCH_CHECK(ctx);
         k_tet_sort_emit<<<blocks_for(n, 128), 128, 0, s>>>(n, toff, keys, eoff, ER, orig,
                                                            out.d_tets);

@@ -457,3 +457,27 @@ def test_engine_matches_plain_reference_binary(pac, name):
         r = eng.alpha_complex(balls, man["sol_rad"], man["alpha"])
     _same(r, *_refrun(name, "plain-rr128-nofma"))
 
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_passes_partition_the_complex(pac, orc, world):
+    """The engine's slab passes (Engine(slab=(r, world)), one after the other
+    on this GPU): each equals the restatement's simplices owned by the slab
+    (pac.slab_cuts, the ownership rule the multi-rank gather relies on), and
+    together in rank order they are the single pass's lists."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_multirank import slab_expectation
+    balls = pac.assembly(nx=2, ny=2, nz=2, per=2500)
+    full, shares = slab_expectation(pac, orc, balls, 1.4, 1.0, world)
+    with _engine(pac) as eng:
+        one = eng.alpha_complex(balls, 1.4, 1.0)
+    _same(one, *full)
+    cat = [[], [], []]
+    for r in range(world):
+        with pac.Engine(tet_mode="as-written", slab=(r, world)) as eng:
+            part = eng.alpha_complex(balls, 1.4, 1.0)
+        _same(part, *shares[r])
+        for k, a in enumerate((part.edges, part.tris, part.tets)):
+            cat[k].append(a)
+    _same(pac.Result(*[np.concatenate(c) for c in cat], None), one.edges, one.tris, one.tets)
