@@ -254,6 +254,10 @@ def main():
     ap.add_argument("--n", type=int, default=N_BALLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-molecules", type=int, default=4096)
+    ap.add_argument("--queue-entries", type=int, default=0,
+                    help="cap the alpha-tetrahedron queue (32 B entries; default: a quarter "
+                         "of free device memory, at most 12 GiB), e.g. to keep a profiled "
+                         "run's device memory small")
     ap.add_argument("--no-exact", action="store_true",
                     help="skip the decision-exact (precision cascade) measurements")
     ap.add_argument("--no-assembly", action="store_true",
@@ -280,7 +284,8 @@ def main():
     # centre then lies inside the grid, so the reference can run this input
     balls = pac.pad_corners(pac.globule(n, seed=pac.SEED_BASE + 4 + 1000 * rank))
     n = len(balls)
-    eng = pac.Engine(device=local, formula="upstream", tet_mode="as-written", predicates="strict")
+    eng = pac.Engine(device=local, formula="upstream", tet_mode="as-written", predicates="strict",
+                     queue_entries=args.queue_entries or None)
     d_balls = torch.from_numpy(balls).cuda()
     torch.cuda.synchronize()  # the engine's stream does not wait on torch's
     stream = torch.cuda.ExternalStream(eng.stream())
