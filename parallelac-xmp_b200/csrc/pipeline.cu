@@ -2293,6 +2293,18 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         };
         unsigned long long cand_total = 0, alpha_total = 0;
         uint64_t lo = work_lo, chunk = n;
+        {
+            // first chunk: the whole range when its queue demand (a few
+            // entries per alpha triangle) clearly fits, else a probe of 1/32
+            // whose fill sizes the next chunks -- an overflowing chunk is
+            // enumerated again, smaller
+            unsigned long long atri = 0;
+            CK(cudaMemcpyAsync(&atri, ctr + C_ALPHA_T, sizeof(atri), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            const double span = (double)(own_hi - work_lo), share = span / (double)std::max<uint64_t>(1, n);
+            if (2.0 * (double)atri * share > 0.85 * (double)qcap)
+                chunk = std::max<uint64_t>(1, (uint64_t)(span / 32.0));
+        }
         // verbose: per-chunk enumeration and scan times
         cudaEvent_t vev[3] = {nullptr, nullptr, nullptr};
         if (cfg.verbose)
