@@ -1042,6 +1042,7 @@ struct EnumSmem<1> {
     uint16_t cand[kWarps][kCandCap];  // (b-chunk index j) | c << 8
     uint8_t sBl[kWarps][kDeg];    // the b's of the row, ascending
     unsigned long long best[kWarps][64];  // per (j, side): orderable key << 32 | c
+    pac::TetGroup grp[kWarps][32];        // markRealTets' products of the chunk's groups
 };
 // larger balls: rows read in place, v2's rows staged when they fit
 template <>
@@ -1055,6 +1056,7 @@ struct EnumSmem<kMaxW> {
     uint16_t cand[kWarps][kCandCap];
     uint8_t sBl[kWarps][kDeg];
     unsigned long long best[kWarps][64];
+    pac::TetGroup grp[kWarps][32];
 };
 
 // Per-warp state of the queue reservation.
@@ -1179,6 +1181,10 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         if (lane < nj) {
             const int b = sBl[k0 + lane];
             const int mb = smap[b];  // 0xffff: (v2, v3) has no alpha edge in v2's list
+            if constexpr (V != pac::kExact) {
+                const float4 b3 = sb[b];
+                S.grp[wib][lane] = pac::tet_group(B1, B2, Ball{b3.x, b3.y, b3.z, b3.w});
+            }
 #pragma unroll
             for (int w = 0; w < KW; w++)
                 pm[w] = (w < W && mb != 0xffff) ? (ra[w] & L[(uint64_t)b * W + w] & above_mask(b, w))
@@ -1248,7 +1254,10 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
                     const float4 b3 = sb[b], b4 = sb[c];
                     B3 = Ball{b3.x, b3.y, b3.z, b3.w};
                     B4 = Ball{b4.x, b4.y, b4.z, b4.w};
-                    passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
+                    if constexpr (V == pac::kExact)
+                        passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
+                    else
+                        passA = pac::tet_alpha_g(S.grp[wib][j], B2, B3, B4, A.alpha, sphere);
                     if (passA) {
                         // the triangle (p, v2, v3)'s normal; the side of v4
                         // and the pencil position of the orthocentre

@@ -159,6 +159,76 @@ __device__ __forceinline__ bool tet_alpha(const Ball a1, const Ball a2, const Ba
     return le_as_double(dist, alpha);
 }
 
+// markRealTets in two parts, for the enumeration, where the tetrahedra of
+// one triangle group (a1, a2, a3) differ only in a4.  Every product of the
+// reference's determinants (LD:569-576) multiplies two factors that depend
+// on a1, a2, a3 only, then one that involves a4: ((f * g) * h).  TetGroup
+// holds the twelve (f * g) of a group, computed once by the same operations;
+// tet_alpha_g completes a tetrahedron from them with the same operations in
+// the same order, so its results are those of tet_alpha bit for bit.
+struct TetGroup {
+    float p11_22, p12_23, p13_21, p13_22, p12_21, p11_23;  // a1i * a2j
+    float pb1_22, p13_b2, p12_b2, pb1_23, p11_b2, pb1_21;  // with b1, b2
+};
+
+__device__ __forceinline__ TetGroup tet_group(const Ball a1, const Ball a2, const Ball a3) {
+    float a11 = a1.x - a2.x;
+    float a12 = a1.y - a2.y;
+    float a13 = a1.z - a2.z;
+    float b1 = (a1.x * a1.x - a2.x * a2.x) + (a1.y * a1.y - a2.y * a2.y) +
+               (a1.z * a1.z - a2.z * a2.z) - (a1.r * a1.r) + (a2.r * a2.r);
+    b1 /= 2;
+    float a21 = a2.x - a3.x;
+    float a22 = a2.y - a3.y;
+    float a23 = a2.z - a3.z;
+    float b2 = (a2.x * a2.x - a3.x * a3.x) + (a2.y * a2.y - a3.y * a3.y) +
+               (a2.z * a2.z - a3.z * a3.z) - (a2.r * a2.r) + (a3.r * a3.r);
+    b2 /= 2;
+    TetGroup g;
+    g.p11_22 = a11 * a22;
+    g.p12_23 = a12 * a23;
+    g.p13_21 = a13 * a21;
+    g.p13_22 = a13 * a22;
+    g.p12_21 = a12 * a21;
+    g.p11_23 = a11 * a23;
+    g.pb1_22 = b1 * a22;
+    g.p13_b2 = a13 * b2;
+    g.p12_b2 = a12 * b2;
+    g.pb1_23 = b1 * a23;
+    g.p11_b2 = a11 * b2;
+    g.pb1_21 = b1 * a21;
+    return g;
+}
+
+__device__ __forceinline__ bool tet_alpha_g(const TetGroup &g, const Ball a2, const Ball a3,
+                                            const Ball a4, float alpha, float4 &ortho) {
+    float a31 = a3.x - a4.x;
+    float a32 = a3.y - a4.y;
+    float a33 = a3.z - a4.z;
+    float b3 = (a3.x * a3.x - a4.x * a4.x) + (a3.y * a3.y - a4.y * a4.y) +
+               (a3.z * a3.z - a4.z * a4.z) - (a3.r * a3.r) + (a4.r * a4.r);
+    b3 /= 2;
+    float D = g.p11_22 * a33 + g.p12_23 * a31 + g.p13_21 * a32 - g.p13_22 * a31 -
+              g.p12_21 * a33 - g.p11_23 * a32;
+    float Dx = g.pb1_22 * a33 + g.p12_23 * b3 + g.p13_b2 * a32 - g.p13_22 * b3 -
+               g.p12_b2 * a33 - g.pb1_23 * a32;
+    float Dy = g.p11_b2 * a33 + g.pb1_23 * a31 + g.p13_21 * b3 - g.p13_b2 * a31 -
+               g.pb1_21 * a33 - g.p11_23 * b3;
+    float Dz = g.p11_22 * b3 + g.p12_b2 * a31 + g.pb1_21 * a32 - g.pb1_22 * a31 -
+               g.p12_21 * b3 - g.p11_b2 * a32;
+    if (D == 0.0) {
+        ortho = make_float4(0, 0, 0, 0);
+        return true;
+    }
+    float X = Dx / D;
+    float Y = Dy / D;
+    float Z = Dz / D;
+    float dist = (a2.x - X) * (a2.x - X) + (a2.y - Y) * (a2.y - Y) + (a2.z - Z) * (a2.z - Z) -
+                 a2.r * a2.r;
+    ortho = make_float4(X, Y, Z, dist);
+    return le_as_double(dist, alpha);
+}
+
 // orient3d determinant (PRED:2015-2045); the error bound there is dead.
 __device__ __forceinline__ float orient3d(const float *pa, const float *pb, const float *pc,
                                           const float *pd) {
