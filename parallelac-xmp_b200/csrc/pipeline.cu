@@ -123,6 +123,42 @@ __device__ __forceinline__ int select_bit(const uint64_t *m, int W, int k) {
     }
     return -1;
 }
+// position of the k-th set bit (0-based) of x, k < popcount(x): halve the
+// word by popcounts
+__device__ __forceinline__ int select64(uint64_t x, int k) {
+    uint32_t v = (uint32_t)x;
+    int pos = 0;
+    const int pl = __popc(v);
+    if (k >= pl) {
+        k -= pl;
+        v = (uint32_t)(x >> 32);
+        pos = 32;
+    }
+    int q = __popc(v & 0xffffu);
+    if (k >= q) k -= q, v >>= 16, pos += 16;
+    q = __popc(v & 0xffu);
+    if (k >= q) k -= q, v >>= 8, pos += 8;
+    q = __popc(v & 0xfu);
+    if (k >= q) k -= q, v >>= 4, pos += 4;
+    q = __popc(v & 0x3u);
+    if (k >= q) k -= q, v >>= 2, pos += 2;
+    return pos + (k >= (int)(v & 1u) ? 1 : 0);
+}
+// the same over a KW-word mask, k < its popcount
+template <int KW>
+__device__ __forceinline__ int select_kw(const uint64_t *m, int k) {
+    int w = 0;
+    uint64_t x = m[0];
+#pragma unroll
+    for (int v = 0; v + 1 < KW; v++) {
+        const int q = __popcll(x);
+        if (k < q) break;
+        k -= q;
+        w = v + 1;
+        x = m[v + 1];
+    }
+    return w * 64 + select64(x, k);
+}
 // bits of word w whose global position is greater than b
 __device__ __forceinline__ uint64_t above_mask(int b, int w) {
     if (w * 64 + 63 <= b) return 0ull;
@@ -1032,14 +1068,15 @@ struct EnumSmem;
 // balls of at most 64 upper neighbours: one link word per row, all staged
 template <>
 struct EnumSmem<1> {
-    static constexpr int kDeg = 64, kL2Cap = 64, kCandCap = 256, kWarps = 8;
+    static constexpr int kDeg = 64, kL2Cap = 64, kWarps = 8;
     float4 sb[kWarps][kDeg];      // balls of p's upper neighbours
     uint64_t sL[kWarps][kDeg];    // p's link rows
     uint64_t sL2[kWarps][kL2Cap]; // v2's link rows (when they fit)
     uint32_t sN2[kWarps][kMaxDeg];// v2's upper neighbours
     uint32_t sN[kWarps][kDeg];    // p's upper neighbours
     uint16_t smap[kWarps][kDeg];  // position of N[c] in v2's list, 0xffff: absent
-    uint16_t cand[kWarps][kCandCap];  // (b-chunk index j) | c << 8
+    uint64_t pm[kWarps][32][1];   // the chunk's groups' fourth vertices (bits c)
+    uint8_t gstart[kWarps][32];   // group starting at each slot of a batch
     uint8_t sBl[kWarps][kDeg];    // the b's of the row, ascending
     unsigned long long best[kWarps][64];  // per (j, side): orderable key << 32 | c
     pac::TetGroup grp[kWarps][32];        // markRealTets' products of the chunk's groups
@@ -1047,13 +1084,14 @@ struct EnumSmem<1> {
 // larger balls: rows read in place, v2's rows staged when they fit
 template <>
 struct EnumSmem<kMaxW> {
-    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kCandCap = 512, kWarps = 4;
+    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kWarps = 4;
     float4 sb[kWarps][kDeg];
     uint64_t sL2[kWarps][kL2Cap];
     uint32_t sN2[kWarps][kMaxDeg];
     uint32_t sN[kWarps][kDeg];
     uint16_t smap[kWarps][kDeg];
-    uint16_t cand[kWarps][kCandCap];
+    uint64_t pm[kWarps][32][kMaxW];
+    uint8_t gstart[kWarps][32];
     uint8_t sBl[kWarps][kDeg];
     unsigned long long best[kWarps][64];
     pac::TetGroup grp[kWarps][32];
@@ -1110,7 +1148,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
                                         bool refute, unsigned long long &cand_acc,
                                         unsigned long long &alpha_acc, unsigned long long &kill_acc,
                                         unsigned long long &ktest_acc, Tally &tally) {
-    constexpr int kL2Cap = EnumSmem<KW>::kL2Cap, kCandCap = EnumSmem<KW>::kCandCap;
+    constexpr int kL2Cap = EnumSmem<KW>::kL2Cap;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
     const uint32_t *N = S.sN[wib];
@@ -1208,107 +1246,100 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         S.best[wib][lane] = ~0ull;
         S.best[wib][lane + 32] = ~0ull;
         const int myoff = incl - cnt;
-        // the chunk's candidates, group by group, kCandCap at a time
-        for (int base = 0; base < total; base += kCandCap) {
-            __syncwarp();
-            {
-                int idx = myoff;
 #pragma unroll
-                for (int w = 0; w < KW; w++) {
-                    uint64_t bits = pm[w];
-                    while (bits) {
-                        const int c = w * 64 + __ffsll((long long)bits) - 1;
-                        bits &= bits - 1;
-                        if (idx >= base && idx < base + kCandCap)
-                            S.cand[wib][idx - base] = (uint16_t)(lane | (c << 8));
-                        idx++;
-                    }
+        for (int w = 0; w < KW; w++) S.pm[wib][lane][w] = pm[w];
+        // the chunk's candidates in group order, 32 per batch: slot t holds
+        // the r-th fourth vertex of group j, t = start(j) + r.  A batch finds
+        // its slots' groups from the mask of the group starts inside it; a
+        // slot before the first start continues the previous batch's last
+        // group.
+        int jcarry = 0;
+        for (int s0 = 0; s0 < total; s0 += 32) {
+            __syncwarp();
+            const int rel = myoff - s0;
+            const bool starts = cnt > 0 && rel >= 0 && rel < 32;
+            if (starts) S.gstart[wib][rel] = (uint8_t)lane;
+            const unsigned M = __reduce_or_sync(kFull, starts ? 1u << rel : 0u);
+            __syncwarp();
+            const unsigned upto = M & (0xffffffffu >> (31 - lane));
+            const int j = upto ? (int)S.gstart[wib][31 - __clz(upto)] : jcarry;
+            jcarry = __shfl_sync(kFull, j, 31);
+            const int r = s0 + lane - __shfl_sync(kFull, myoff, j);
+            const bool act = s0 + lane < total;
+            const int c = act ? select_kw<KW>(S.pm[wib][j], r) : 0;
+            const int b = act ? (int)sBl[k0 + j] : 0;
+            bool face = false;
+            if (act) {  // (v2, v3, v4) an alpha triangle: bit of v2's link
+                const int mb = smap[b], mc = smap[c];
+                if (mc != 0xffff) {
+                    const uint64_t at2 = (uint64_t)mb * W2 + (mc >> 6);
+                    face = ((l2s ? sL2[at2] : __ldg(&L2g[at2])) >> (mc & 63)) & 1ull;
                 }
             }
-            __syncwarp();
-            const int nwin = min(kCandCap, total - base);
-            for (int s0 = 0; s0 < nwin; s0 += 32) {
-                const bool act = s0 + lane < nwin;
-                int j = 0, c = 0;
-                if (act) {
-                    const uint32_t e = S.cand[wib][s0 + lane];
-                    j = (int)(e & 0xff);
-                    c = (int)(e >> 8);
+            const unsigned mF = __ballot_sync(kFull, face);
+            if (lane == 0) cand_acc += __popc(mF);
+            bool passA = false, side = false;
+            float4 sphere = make_float4(0.f, 0.f, 0.f, 0.f);
+            float key = 0.f;
+            Ball B3{0.f, 0.f, 0.f, 0.f}, B4{0.f, 0.f, 0.f, 0.f};
+            if (face) {
+                const float4 b3 = sb[b], b4 = sb[c];
+                B3 = Ball{b3.x, b3.y, b3.z, b3.w};
+                B4 = Ball{b4.x, b4.y, b4.z, b4.w};
+                if constexpr (V == pac::kExact)
+                    passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
+                else
+                    passA = pac::tet_alpha_g(S.grp[wib][j], B2, B3, B4, A.alpha, sphere);
+                if (passA) {
+                    // the triangle (p, v2, v3)'s normal; the side of v4
+                    // and the pencil position of the orthocentre
+                    const float e13x = B3.x - B1.x, e13y = B3.y - B1.y, e13z = B3.z - B1.z;
+                    const float nx = e12y * e13z - e12z * e13y;
+                    const float ny = e12z * e13x - e12x * e13z;
+                    const float nz = e12x * e13y - e12y * e13x;
+                    side = nx * (B4.x - B1.x) + ny * (B4.y - B1.y) + nz * (B4.z - B1.z) > 0.f;
+                    key = nx * sphere.x + ny * sphere.y + nz * sphere.z;
+                    if (!side) key = -key;
                 }
-                const int b = act ? (int)sBl[k0 + j] : 0;
-                bool face = false;
-                if (act) {  // (v2, v3, v4) an alpha triangle: bit of v2's link
-                    const int mb = smap[b], mc = smap[c];
-                    if (mc != 0xffff) {
-                        const uint64_t at2 = (uint64_t)mb * W2 + (mc >> 6);
-                        face = ((l2s ? sL2[at2] : __ldg(&L2g[at2])) >> (mc & 63)) & 1ull;
-                    }
+            }
+            const unsigned mA = __ballot_sync(kFull, passA);
+            if (lane == 0) alpha_acc += __popc(mA);
+            bool keep = passA;
+            if constexpr (V != pac::kExact) {
+                // the flat tetrahedra (orthocentre 0, LD:577-580) and
+                // non-finite keys take no part
+                const bool cand_best = refute && passA && isfinite(key) &&
+                                       !(sphere.x == 0.f && sphere.y == 0.f && sphere.z == 0.f);
+                const int slot = j + (side ? 32 : 0);
+                if (cand_best) {
+                    const uint32_t kb = __float_as_uint(key);
+                    const uint32_t ok = (kb & 0x80000000u) ? ~kb : (kb | 0x80000000u);
+                    atomicMin(&S.best[wib][slot], ((unsigned long long)ok << 32) | (uint32_t)c);
                 }
-                const unsigned mF = __ballot_sync(kFull, face);
-                if (lane == 0) cand_acc += __popc(mF);
-                bool passA = false, side = false;
-                float4 sphere = make_float4(0.f, 0.f, 0.f, 0.f);
-                float key = 0.f;
-                Ball B3{0.f, 0.f, 0.f, 0.f}, B4{0.f, 0.f, 0.f, 0.f};
-                if (face) {
-                    const float4 b3 = sb[b], b4 = sb[c];
-                    B3 = Ball{b3.x, b3.y, b3.z, b3.w};
-                    B4 = Ball{b4.x, b4.y, b4.z, b4.w};
-                    if constexpr (V == pac::kExact)
-                        passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
-                    else
-                        passA = pac::tet_alpha_g(S.grp[wib][j], B2, B3, B4, A.alpha, sphere);
-                    if (passA) {
-                        // the triangle (p, v2, v3)'s normal; the side of v4
-                        // and the pencil position of the orthocentre
-                        const float e13x = B3.x - B1.x, e13y = B3.y - B1.y, e13z = B3.z - B1.z;
-                        const float nx = e12y * e13z - e12z * e13y;
-                        const float ny = e12z * e13x - e12x * e13z;
-                        const float nz = e12x * e13y - e12y * e13x;
-                        side = nx * (B4.x - B1.x) + ny * (B4.y - B1.y) + nz * (B4.z - B1.z) > 0.f;
-                        key = nx * sphere.x + ny * sphere.y + nz * sphere.z;
-                        if (!side) key = -key;
-                    }
-                }
-                const unsigned mA = __ballot_sync(kFull, passA);
-                if (lane == 0) alpha_acc += __popc(mA);
-                bool keep = passA;
-                if constexpr (V != pac::kExact) {
-                    // the flat tetrahedra (orthocentre 0, LD:577-580) and
-                    // non-finite keys take no part
-                    const bool cand_best = refute && passA && isfinite(key) &&
-                                           !(sphere.x == 0.f && sphere.y == 0.f && sphere.z == 0.f);
-                    const int slot = j + (side ? 32 : 0);
-                    if (cand_best) {
-                        const uint32_t kb = __float_as_uint(key);
-                        const uint32_t ok = (kb & 0x80000000u) ? ~kb : (kb | 0x80000000u);
-                        atomicMin(&S.best[wib][slot], ((unsigned long long)ok << 32) | (uint32_t)c);
-                    }
-                    __syncwarp();
-                    if (cand_best) {
-                        const int y = (int)(S.best[wib][slot] & 0xffffffffull);
-                        const float4 by = sb[y];
-                        if (y != c && surely_in_window(sphere.x, sphere.y, sphere.z, by.x, by.y, by.z,
-                                                       0.99f * G.step)) {
-                            float pa[3] = {B1.x, B1.y, B1.z}, pb[3] = {B2.x, B2.y, B2.z};
-                            float pc[3] = {B3.x, B3.y, B3.z}, pd[3] = {B4.x, B4.y, B4.z};
-                            float pe[3] = {by.x, by.y, by.z};
-                            const float wa = wt<V>(B1.r), wb = wt<V>(B2.r), wc = wt<V>(B3.r),
-                                        wd = wt<V>(B4.r);
-                            const float ori = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
-                            const float res = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd,
-                                                              wt<V>(by.w), tally);
-                            ktest_acc++;
-                            if (ori < 0 ? (res < 0) : (res > 0)) {
-                                keep = false;
-                                kill_acc++;
-                            }
+                __syncwarp();
+                if (cand_best) {
+                    const int y = (int)(S.best[wib][slot] & 0xffffffffull);
+                    const float4 by = sb[y];
+                    if (y != c && surely_in_window(sphere.x, sphere.y, sphere.z, by.x, by.y, by.z,
+                                                   0.99f * G.step)) {
+                        float pa[3] = {B1.x, B1.y, B1.z}, pb[3] = {B2.x, B2.y, B2.z};
+                        float pc[3] = {B3.x, B3.y, B3.z}, pd[3] = {B4.x, B4.y, B4.z};
+                        float pe[3] = {by.x, by.y, by.z};
+                        const float wa = wt<V>(B1.r), wb = wt<V>(B2.r), wc = wt<V>(B3.r),
+                                    wd = wt<V>(B4.r);
+                        const float ori = dec_orient<V>(pa, pb, pc, pd, wa, wb, wc, wd, tally);
+                        const float res = dec_insphere<V>(pa, pb, pc, pd, pe, wa, wb, wc, wd,
+                                                          wt<V>(by.w), tally);
+                        ktest_acc++;
+                        if (ori < 0 ? (res < 0) : (res > 0)) {
+                            keep = false;
+                            kill_acc++;
                         }
                     }
                 }
-                queue_append(Q, A.ctr, qr, keep,
-                             make_uint4(p, v2, act ? N[b] : 0u, act ? N[c] : 0u), sphere);
             }
+            queue_append(Q, A.ctr, qr, keep,
+                         make_uint4(p, v2, act ? N[b] : 0u, act ? N[c] : 0u), sphere);
         }
         __syncwarp();
     }
