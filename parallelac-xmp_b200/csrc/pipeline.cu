@@ -1068,11 +1068,14 @@ struct EnumSmem;
 // balls of at most 64 upper neighbours: one link word per row, all staged
 template <>
 struct EnumSmem<1> {
-    static constexpr int kDeg = 64, kL2Cap = 64, kWarps = 8;
+    static constexpr int kDeg = 64, kL2Cap = 64, kWarps = 8, kBufs = 2;
     float4 sb[kWarps][kDeg];      // balls of p's upper neighbours
     uint64_t sL[kWarps][kDeg];    // p's link rows
-    uint64_t sL2[kWarps][kL2Cap]; // v2's link rows (when they fit)
-    uint32_t sN2[kWarps][kMaxDeg];// v2's upper neighbours
+    uint64_t sL2[kWarps][kBufs][kL2Cap]; // v2's link rows (when they fit), this row and the next
+    uint32_t sN2[kWarps][kBufs][kMaxDeg];// v2's upper neighbours, this row and the next
+    uint64_t sE2[kWarps][kDeg];   // per neighbour v2: its first upper neighbour's index,
+    uint64_t sLo[kWarps][kDeg];   // its link rows' offset,
+    uint16_t sD2[kWarps][kDeg];   // its upper degree
     uint32_t sN[kWarps][kDeg];    // p's upper neighbours
     uint16_t smap[kWarps][kDeg];  // position of N[c] in v2's list, 0xffff: absent
     uint64_t pm[kWarps][32][1];   // the chunk's groups' fourth vertices (bits c)
@@ -1084,10 +1087,10 @@ struct EnumSmem<1> {
 // larger balls: rows read in place, v2's rows staged when they fit
 template <>
 struct EnumSmem<kMaxW> {
-    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kWarps = 4;
+    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kWarps = 4, kBufs = 1;
     float4 sb[kWarps][kDeg];
-    uint64_t sL2[kWarps][kL2Cap];
-    uint32_t sN2[kWarps][kMaxDeg];
+    uint64_t sL2[kWarps][kBufs][kL2Cap];
+    uint32_t sN2[kWarps][kBufs][kMaxDeg];
     uint32_t sN[kWarps][kDeg];
     uint16_t smap[kWarps][kDeg];
     uint64_t pm[kWarps][32][kMaxW];
@@ -1138,12 +1141,46 @@ __device__ __forceinline__ void queue_close(const TetQueue &Q, QRes &qr) {
     qr.pos = qr.end;
 }
 
+// Asynchronous global -> shared copies (cp.async): the row after the
+// current one is fetched while the current one is worked on.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Starts copying row a's v2 (upper neighbours and, when they fit, link
+// rows) into buffer buf of the warp's staging (KW = 1), as one cp.async
+// group of this thread.
+__device__ __forceinline__ void row_fetch(const TetArgs &A, EnumSmem<1> &S, int wib, int a,
+                                          int buf) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t e2 = S.sE2[wib][a];
+    const int deg2 = S.sD2[wib][a];
+    const int W2 = (deg2 + 63) >> 6;
+    for (int k = lane; k < deg2; k += 32) cp_async4(&S.sN2[wib][buf][k], &A.ER[e2 + k]);
+    if (deg2 * W2 <= EnumSmem<1>::kL2Cap) {
+        const uint64_t *L2g = A.link + S.sLo[wib][a];
+        for (int k = lane; k < deg2 * W2; k += 32) cp_async8(&S.sL2[wib][buf][k], &L2g[k]);
+    }
+    cp_async_commit();
+}
+
 // One row a of ball p: v2 = N[a].  N, sb, sCell hold p's upper neighbours,
 // their balls and cells (shared memory); L its link rows (W words each,
 // shared or global); the rest is per-warp scratch.
 template <int V, int KW>
 __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, EnumSmem<KW> &S,
-                                        const int wib, QRes &qr, uint32_t p, int a, int deg, int W,
+                                        const int wib, QRes &qr, uint32_t p, int a, int buf,
+                                        int deg, int W,
                                         const uint64_t *L, const Ball B1, const MolGrid &G,
                                         bool refute, unsigned long long &cand_acc,
                                         unsigned long long &alpha_acc, unsigned long long &kill_acc,
@@ -1162,18 +1199,28 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
     }
     if (nb < 2) return;
     const uint32_t v2 = N[a];
-    const uint64_t e2 = A.eoff[v2];
-    const int deg2 = (int)(A.eoff[v2 + 1] - e2);
-    const int W2 = (deg2 + 63) >> 6;
-    const uint64_t *L2g = A.link + A.loff[v2];
-    const bool l2s = deg2 * W2 <= kL2Cap;
-    uint32_t *sN2 = S.sN2[wib];
-    uint64_t *sL2 = S.sL2[wib];
+    uint32_t *sN2 = S.sN2[wib][buf];
+    uint64_t *sL2 = S.sL2[wib][buf];
     uint16_t *smap = S.smap[wib];
     uint8_t *sBl = S.sBl[wib];
-    for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
-    if (l2s)
-        for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2g[k];
+    int deg2;
+    const uint64_t *L2g;
+    if constexpr (KW == 1) {
+        // v2's lists were copied into buffer buf by row_fetch
+        deg2 = S.sD2[wib][a];
+        L2g = A.link + S.sLo[wib][a];
+    } else {
+        const uint64_t e2 = A.eoff[v2];
+        deg2 = (int)(A.eoff[v2 + 1] - e2);
+        L2g = A.link + A.loff[v2];
+        for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
+    }
+    const int W2 = (deg2 + 63) >> 6;
+    const bool l2s = deg2 * W2 <= kL2Cap;
+    if constexpr (KW != 1) {
+        if (l2s)
+            for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2g[k];
+    }
     // the b's of the row, ascending
 #pragma unroll
     for (int w = 0; w < KW; w++) {
@@ -1398,18 +1445,50 @@ __global__ void __launch_bounds__(EnumSmem<KW>::kWarps * 32, KW == 1 ? 3 : 4)
             const uint32_t x = __ldg(&Ng[c]);
             S.sN[wib][c] = x;
             S.sb[wib][c] = __ldg(&A.at[x]);
-
-            if constexpr (KW == 1) S.sL[wib][c] = Lg[c];
+            if constexpr (KW == 1) {
+                S.sL[wib][c] = Lg[c];
+                const uint64_t e2 = A.eoff[x];
+                S.sE2[wib][c] = e2;
+                S.sD2[wib][c] = (uint16_t)(A.eoff[x + 1] - e2);
+                S.sLo[wib][c] = A.loff[x];
+            }
         }
         const Ball B1 = pac::ld_ball(&A.at[p]);
         __syncwarp();
-        const uint64_t *L;
-        if constexpr (KW == 1) L = S.sL[wib];
-        else L = Lg;
-        const int a1 = KW == 1 ? deg - 2 : min(a0 + A.unit_rows, deg - 2);
-        for (int a = a0; a < a1; a++)
-            tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, deg, W, L, B1, G, refute, cand_acc,
-                           alpha_acc, kill_acc, ktest_acc, tally);
+        if constexpr (KW == 1) {
+            // the rows with at least two link bits, each one's v2 fetched
+            // while the one before it is worked on
+            const int a1 = deg - 2;
+            uint64_t rows = 0;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int a = 32 * h + lane;
+                const bool use = a < a1 && __popcll(S.sL[wib][a]) >= 2;
+                rows |= (uint64_t)__ballot_sync(kFull, use) << (32 * h);
+            }
+            int buf = 0;
+            if (rows) row_fetch(A, S, wib, __ffsll((long long)rows) - 1, 0);
+            while (rows) {
+                const int a = __ffsll((long long)rows) - 1;
+                rows &= rows - 1;
+                if (rows) {
+                    row_fetch(A, S, wib, __ffsll((long long)rows) - 1, buf ^ 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncwarp();
+                tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, buf, deg, W, S.sL[wib], B1, G,
+                               refute, cand_acc, alpha_acc, kill_acc, ktest_acc, tally);
+                __syncwarp();
+                buf ^= 1;
+            }
+        } else {
+            const int a1 = min(a0 + A.unit_rows, deg - 2);
+            for (int a = a0; a < a1; a++)
+                tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, 0, deg, W, Lg, B1, G, refute,
+                               cand_acc, alpha_acc, kill_acc, ktest_acc, tally);
+        }
         __syncwarp();
     }
     queue_close(Q, qr);
