@@ -1569,6 +1569,10 @@ __global__ void __launch_bounds__(256, 4) k_tets_scan(TetArgs A, TetQueue Q, uin
             head = b;
             tail = min(nq, b + (uint64_t)A.scan_claim);
             if (head >= tail) more = false;
+            for (uint64_t k = head + 4 * lane; k < tail; k += 128) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(Q.vid + k));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(Q.sph + k));
+            }
         }
         if (want && head < tail) {
             const int r = __popc(want & lt_mask);
