@@ -1365,7 +1365,14 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
                 }
                 __syncwarp();
                 if (cand_best) {
-                    const int y = (int)(S.best[wib][slot] & 0xffffffffull);
+                    int y = (int)(S.best[wib][slot] & 0xffffffffull);
+                    if (y == c) {
+                        // the best so far of its side: the other side's
+                        // best so far refutes it unless the triangle's two
+                        // sides are in pencil order
+                        const unsigned long long o = S.best[wib][slot ^ 32];
+                        if (o != ~0ull) y = (int)(o & 0xffffffffull);
+                    }
                     const float4 by = sb[y];
                     if (y != c && surely_in_window(sphere.x, sphere.y, sphere.z, by.x, by.y, by.z,
                                                    0.99f * G.step)) {
