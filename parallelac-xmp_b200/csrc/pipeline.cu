@@ -1329,15 +1329,19 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
             float4 sphere = make_float4(0.f, 0.f, 0.f, 0.f);
             float key = 0.f;
             Ball B3{0.f, 0.f, 0.f, 0.f}, B4{0.f, 0.f, 0.f, 0.f};
-            if (face) {
+            // markRealTets for every candidate, the alpha tetrahedra being
+            // those with the face (v2, v3, v4): a candidate without it, or
+            // outside alpha, can still refute the others (exact mode: the
+            // alpha tetrahedra only)
+            if (V == pac::kExact ? face : act) {
                 const float4 b3 = sb[b], b4 = sb[c];
                 B3 = Ball{b3.x, b3.y, b3.z, b3.w};
                 B4 = Ball{b4.x, b4.y, b4.z, b4.w};
                 if constexpr (V == pac::kExact)
                     passA = dec_tet<V>(B1, B2, B3, B4, A.alpha, sphere, tally);
                 else
-                    passA = pac::tet_alpha_g(S.grp[wib][j], B2, B3, B4, A.alpha, sphere);
-                if (passA) {
+                    passA = pac::tet_alpha_g(S.grp[wib][j], B2, B3, B4, A.alpha, sphere) && face;
+                {
                     // the triangle (p, v2, v3)'s normal; the side of v4
                     // and the pencil position of the orthocentre
                     const float e13x = B3.x - B1.x, e13y = B3.y - B1.y, e13z = B3.z - B1.z;
@@ -1355,10 +1359,11 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
             if constexpr (V != pac::kExact) {
                 // the flat tetrahedra (orthocentre 0, LD:577-580) and
                 // non-finite keys take no part
-                const bool cand_best = refute && passA && isfinite(key) &&
-                                       !(sphere.x == 0.f && sphere.y == 0.f && sphere.z == 0.f);
+                const bool suspect = refute && act && isfinite(key) &&
+                                     !(sphere.x == 0.f && sphere.y == 0.f && sphere.z == 0.f);
+                const bool cand_best = suspect && passA;
                 const int slot = j + (side ? 32 : 0);
-                if (cand_best) {
+                if (suspect) {
                     const uint32_t kb = __float_as_uint(key);
                     const uint32_t ok = (kb & 0x80000000u) ? ~kb : (kb | 0x80000000u);
                     atomicMin(&S.best[wib][slot], ((unsigned long long)ok << 32) | (uint32_t)c);
