@@ -627,11 +627,15 @@ __global__ void __launch_bounds__(256) k_link(uint64_t n, const float4 *__restri
     __shared__ uint64_t srow[8][kMaxW];
     __shared__ uint64_t sL[8][64];  // link rows of a ball of <= 64 upper neighbours
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long cand_acc = 0, alpha_acc = 0;
     Tally tally;
-    for (uint64_t p = warp; p < n; p += nwarps) {
+    // balls handed out by a counter: a warp that finishes a small ball takes
+    // the next one instead of waiting for its block's largest
+    for (;;) {
+        uint64_t p = 0;
+        if (lane == 0) p = atomicAdd(&ctr[C_NEXT], 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= n) break;
         const uint64_t e0 = eoff[p];
         const int deg = (int)(eoff[p + 1] - e0);
         if (deg < 2) continue;
@@ -2337,7 +2341,9 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     uint64_t *link = ar.alloc_n<uint64_t>(nL), *faces = ar.alloc_n<uint64_t>(nL);
     if (!link || !faces) return PAC_ERR_OOM;
     CK(cudaMemsetAsync(faces, 0, sizeof(uint64_t) * (nL ? nL : 1), s));
-    k_link<V><<<warp_blocks(n), 256, 0, s>>>(n, at, eoff, ER, loff, link, in.alpha, ctr);
+    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+    k_link<V><<<std::min<unsigned>(warp_blocks(n), 148 * 4), 256, 0, s>>>(n, at, eoff, ER, loff,
+                                                                          link, in.alpha, ctr);
     LAUNCH_CHECK(ctx);
     tm.mark();  // 3
 
