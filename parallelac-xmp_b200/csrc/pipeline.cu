@@ -1547,6 +1547,7 @@ __global__ void k_heavy_rows(uint64_t n, const uint64_t *eoff, int unit_rows, ui
 }
 
 constexpr int kScanStep = 4;
+constexpr int kScanRefill = 16;  // idle lanes that trigger a refill
 
 // k_tets_scan: the empty-orthosphere test (checkTetsOrthosphere,
 // AlphaComplexLargeData.cu:606-734) of the queued tetrahedra.  Each lane
@@ -1577,7 +1578,10 @@ __global__ void __launch_bounds__(256, 4) k_tets_scan(TetArgs A, TetQueue Q, uin
     const MolGrid *G = A.grids;
     while (true) {
         // claim: idle lanes take the next entries of the warp's range
-        const unsigned want = __ballot_sync(kFull, !have);
+        // idle lanes take new tetrahedra together, once enough of them
+        // wait (or none works): the setup then runs for many lanes at once
+        unsigned want = __ballot_sync(kFull, !have);
+        if (!(__popc(want) >= kScanRefill || want == kFull)) want = 0u;
         if (want && head >= tail && more) {
             uint64_t b = 0;
             if (lane == 0) b = atomicAdd(claim, (unsigned long long)A.scan_claim);
@@ -1833,6 +1837,7 @@ __global__ void k_map4(uint64_t nq, const uint32_t *orig, uint32_t *tets) {
 // as its own is decided.  An unattached triangle sets its bit in `faces`.
 // Then the warp counts v1's final triangles and marks their edges.
 constexpr int kTQCap = 256;
+constexpr int kTARefill = 24;  // idle lanes that trigger a refill
 
 template <int V>
 __global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t p_lo, uint64_t n,
@@ -1914,8 +1919,11 @@ __global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t p_lo, uint64_t n
                     }
                     __syncwarp();
                 }
+                // idle lanes take new triangles together, once enough of
+                // them wait (or none works): the setup runs for many lanes
+                // at a time instead of for a few in every step
                 unsigned want = __ballot_sync(kFull, !have);
-                if (want && head < qn) {
+                if (want && head < qn && (__popc(want) >= kTARefill || want == kFull)) {
                     int r = __popc(want & lt_mask);
                     if (!have && head + r < qn) {
                         ta = qa[wib][head + r];
