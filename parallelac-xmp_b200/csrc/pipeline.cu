@@ -1982,27 +1982,32 @@ __global__ void __launch_bounds__(256, 4) k_tri_attach(uint64_t p_lo, uint64_t n
             }
             __syncwarp();
             __threadfence_block();
-            // count the final triangles and mark their edges
-            for (int a = 0; a < deg - 1; a++) {
+            // count the final triangles and mark their edges: a lane per
+            // row, 32 rows at a time
+            for (int a0 = 0; a0 < deg - 1; a0 += 32) {
+                const int a = a0 + lane;
                 uint64_t fin[kMaxW];
                 int nf = 0;
 #pragma unroll
                 for (int w = 0; w < kMaxW; w++) {
-                    fin[w] = w < W ? faces[lp + (uint64_t)a * W + w] : 0;
+                    fin[w] = (a < deg - 1 && w < W) ? faces[lp + (uint64_t)a * W + w] : 0;
                     nf += __popcll(fin[w]);
                 }
-                count += nf;
+                count += (uint32_t)warp_sum((unsigned long long)nf);
                 if (!nf) continue;
-                if (lane == 0) eflag[e0 + a] = 1;
+                eflag[e0 + a] = 1;
                 const uint32_t va = N[a];
                 const uint64_t e1 = eoff[va];
                 const int deg1 = (int)(eoff[va + 1] - e1);
-                for (int k0 = 0; k0 < nf; k0 += 32) {
-                    int b = (k0 + lane < nf) ? select_bit(fin, W, k0 + lane) : -1;
-                    if (b >= 0) {
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    uint64_t bits = fin[w];
+                    while (bits) {
+                        const int b = w * 64 + __ffsll((long long)bits) - 1;
+                        bits &= bits - 1;
                         eflag[e0 + b] = 1;
                         const uint32_t vb = N[b];
-                        int pos = lbound(ER + e1, deg1, vb);
+                        const int pos = lbound(ER + e1, deg1, vb);
                         if (pos < deg1 && ER[e1 + pos] == vb) eflag[e1 + pos] = 1;
                     }
                 }
@@ -2112,25 +2117,42 @@ __global__ void __launch_bounds__(256) k_emit_tris(uint64_t p_lo, uint64_t n, co
         const int W = (deg + 63) >> 6;
         const uint32_t *N = ER + eoff[p];
         const uint32_t o0 = orig[p];
+        const uint64_t lp = loff[p];
         uint64_t q = tpos[p];
-        for (int a = 0; a < deg - 1; a++) {
+        // a lane per row, 32 rows at a time; rows in order, b ascending
+        // within a row
+        for (int a0 = 0; a0 < deg - 1; a0 += 32) {
+            const int a = a0 + lane;
             uint64_t f[kMaxW];
             int nf = 0;
+#pragma unroll
             for (int w = 0; w < kMaxW; w++) {
-                f[w] = w < W ? faces[loff[p] + (uint64_t)a * W + w] : 0;
+                f[w] = (a < deg - 1 && w < W) ? faces[lp + (uint64_t)a * W + w] : 0;
                 nf += __popcll(f[w]);
             }
-            const uint32_t o1 = orig[N[a]];
-            for (int k0 = 0; k0 < nf; k0 += 32) {
-                int k = k0 + lane;
-                if (k < nf) {
-                    int b = select_bit(f, W, k);
-                    out[3 * (q + k)] = o0;
-                    out[3 * (q + k) + 1] = o1;
-                    out[3 * (q + k) + 2] = orig[N[b]];
+            int incl = nf;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(kFull, incl, 31);
+            if (nf) {
+                const uint32_t o1 = orig[N[a]];
+                uint64_t at = q + (uint64_t)(incl - nf);
+#pragma unroll
+                for (int w = 0; w < kMaxW; w++) {
+                    uint64_t bits = f[w];
+                    while (bits) {
+                        const int b = w * 64 + __ffsll((long long)bits) - 1;
+                        bits &= bits - 1;
+                        out[3 * at] = o0;
+                        out[3 * at + 1] = o1;
+                        out[3 * at + 2] = orig[N[b]];
+                        at++;
+                    }
                 }
             }
-            q += nf;
+            q += (uint64_t)total;
         }
     }
 }
