@@ -2031,11 +2031,14 @@ __global__ void __launch_bounds__(256) k_edge_final(uint64_t p_lo, uint64_t n,
                                                     const uint32_t *mol, const MolGrid *grids,
                                                     unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
-    uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long oob = 0;
     Tally tally;
-    for (uint64_t p = p_lo + warp; p < n; p += nwarps) {
+    // balls handed out by a counter (persistent warps)
+    for (;;) {
+        uint64_t p = 0;
+        if (lane == 0) p = p_lo + atomicAdd(&ctr[C_NEXT], 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= n) break;
         const uint64_t e0 = eoff[p];
         const int deg = (int)(eoff[p + 1] - e0);
         if (!deg) continue;
@@ -2624,8 +2627,9 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         in.alpha, ctr);
     LAUNCH_CHECK(ctx);
     tm.mark();  // 5
-    k_edge_final<V><<<warp_blocks(own_hi - own_lo), 256, 0, s>>>(own_lo, own_hi, at, eoff, ER, eflag,
-                                                                 cellbeg, mol, grids, ctr);
+    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+    k_edge_final<V><<<std::min<unsigned>(warp_blocks(own_hi - own_lo), 148 * 5), 256, 0, s>>>(
+        own_lo, own_hi, at, eoff, ER, eflag, cellbeg, mol, grids, ctr);
     LAUNCH_CHECK(ctx);
     if (cfg.slab_world > 1) {
         // only the owned balls' triangles and edges are output
