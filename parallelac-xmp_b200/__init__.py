@@ -13,6 +13,7 @@ in ``lib/libpac.so``.  There is no Python or CPU fallback: if the library or a
 CUDA device is missing, the calls raise.
 """
 import ctypes
+import time
 import os
 from concurrent.futures import ThreadPoolExecutor
 
@@ -140,18 +141,31 @@ def _check(status):
         raise PacError(status, _lib().pac_last_error().decode())
 
 
+def _copy_many(srcs):
+    """Copies of several arrays, large ones in 32 MB slices spread over the
+    host's threads (numpy releases the GIL while copying; the first touch
+    of the new pages is most of the cost): lists of a batched pass run to
+    gigabytes."""
+    outs = [np.empty_like(a) if a.nbytes >= (16 << 20) else a.copy() for a in srcs]
+    jobs = []
+    for a, o in zip(srcs, outs):
+        if a.nbytes >= (16 << 20):
+            step = max(1, (32 << 20) // a.itemsize)
+            jobs += [(a, o, i, min(len(a), i + step)) for i in range(0, len(a), step)]
+    if jobs:
+        with ThreadPoolExecutor(min(len(jobs), os.cpu_count() or 1, 64)) as ex:
+            list(ex.map(lambda j: np.copyto(j[1][j[2]:j[3]], j[0][j[2]:j[3]]), jobs))
+    return outs
+
+
 def _copy(src):
-    """Copy of a large array, in slices on several threads (numpy releases
-    the GIL while copying): lists of a batched pass run to gigabytes."""
-    if src.nbytes < (16 << 20):
-        return src.copy()
-    out = np.empty_like(src)
-    parts = min(16, os.cpu_count() or 1)
-    step = -(-len(src) // parts)
-    with ThreadPoolExecutor(parts) as ex:
-        list(ex.map(lambda i: np.copyto(out[i * step:(i + 1) * step], src[i * step:(i + 1) * step]),
-                    range(parts)))
-    return out
+    return _copy_many([src])[0]
+
+
+def _view(ptr, count, k):
+    if count == 0:
+        return np.zeros((0,), np.uint32)
+    return np.ctypeslib.as_array(ptr, (count * k,))
 
 
 def _arr(ptr, count, k):
@@ -224,15 +238,21 @@ class Engine:
         """The engine's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
         return _lib().pac_cuda_stream(self._ctx) or 0
 
-    def alpha_complex(self, balls, sol_rad, alpha):
-        """balls: (n, 4) float32 (x, y, z, raw radius) on the host."""
+    def alpha_complex(self, balls, sol_rad, alpha, timing=None):
+        """balls: (n, 4) float32 (x, y, z, raw radius) on the host.
+        timing: optional dict; receives 'c_call_s', the wall time of the C
+        call alone (without this wrapper's copy of the lists)."""
         b = np.ascontiguousarray(balls, dtype=np.float32)
         if b.ndim != 2 or b.shape[1] != 4:
             raise ValueError("balls must have shape (n, 4)")
         cx, st = Complex(), Stats()
-        _check(_lib().pac_alpha_complex(self._ctx, b.ctypes.data_as(ctypes.c_void_p), len(b),
-                                        float(sol_rad), float(alpha), ctypes.byref(cx),
-                                        ctypes.byref(st)))
+        t0 = time.perf_counter()
+        rc = _lib().pac_alpha_complex(self._ctx, b.ctypes.data_as(ctypes.c_void_p), len(b),
+                                      float(sol_rad), float(alpha), ctypes.byref(cx),
+                                      ctypes.byref(st))
+        if timing is not None:
+            timing["c_call_s"] = time.perf_counter() - t0
+        _check(rc)
         try:
             return Result(_arr(cx.edges, cx.n_edges, 2), _arr(cx.tris, cx.n_tris, 3),
                           _arr(cx.tets, cx.n_tets, 4), st.as_dict())
@@ -275,24 +295,30 @@ class Engine:
             ctypes.c_void_p(d_darea_ptr or None)))
         return vol.value, area.value
 
-    def alpha_complex_batch(self, balls, offsets, sol_rad, alpha):
+    def alpha_complex_batch(self, balls, offsets, sol_rad, alpha, timing=None):
         """Many molecules back to back; offsets has n_mol + 1 entries.
-        Returns a list of Result (molecule-local indices) and the stats."""
+        Returns a list of Result (molecule-local indices) and the stats.
+        timing: optional dict; receives 'c_call_s', the wall time of the C
+        call alone (without this wrapper's copy of the lists)."""
         b = np.ascontiguousarray(balls, dtype=np.float32)
         off = np.ascontiguousarray(offsets, dtype=np.uint64)
         nm = len(off) - 1
         bc, st = BatchComplex(), Stats()
-        _check(_lib().pac_alpha_complex_batch(self._ctx, b.ctypes.data_as(ctypes.c_void_p),
-                                              off.ctypes.data_as(ctypes.c_void_p), nm,
-                                              float(sol_rad), float(alpha), ctypes.byref(bc),
-                                              ctypes.byref(st)))
+        t0 = time.perf_counter()
+        rc = _lib().pac_alpha_complex_batch(self._ctx, b.ctypes.data_as(ctypes.c_void_p),
+                                            off.ctypes.data_as(ctypes.c_void_p), nm,
+                                            float(sol_rad), float(alpha), ctypes.byref(bc),
+                                            ctypes.byref(st))
+        if timing is not None:
+            timing["c_call_s"] = time.perf_counter() - t0
+        _check(rc)
         try:
             eo = np.ctypeslib.as_array(bc.edge_off, (nm + 1,)).copy()
             to = np.ctypeslib.as_array(bc.tri_off, (nm + 1,)).copy()
             qo = np.ctypeslib.as_array(bc.tet_off, (nm + 1,)).copy()
-            E = _arr(bc.edges, int(eo[-1]), 2)
-            T = _arr(bc.tris, int(to[-1]), 3)
-            Q = _arr(bc.tets, int(qo[-1]), 4)
+            E, T, Q = _copy_many([_view(bc.edges, int(eo[-1]), 2), _view(bc.tris, int(to[-1]), 3),
+                                  _view(bc.tets, int(qo[-1]), 4)])
+            E, T, Q = E.reshape(-1, 2), T.reshape(-1, 3), Q.reshape(-1, 4)
             res = [Result(E[eo[m]:eo[m + 1]], T[to[m]:to[m + 1]], Q[qo[m]:qo[m + 1]], None)
                    for m in range(nm)]
             return res, st.as_dict()
