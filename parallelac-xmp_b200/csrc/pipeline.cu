@@ -1217,14 +1217,16 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         const uint64_t e2 = A.eoff[v2];
         deg2 = (int)(A.eoff[v2 + 1] - e2);
         L2g = A.link + A.loff[v2];
+        // v2's link rows arrive (cp.async) while its neighbours are staged
+        // and searched below
+        const int W2h = (deg2 + 63) >> 6;
+        if (deg2 * W2h <= kL2Cap)
+            for (int k = lane; k < deg2 * W2h; k += 32) cp_async8(&sL2[k], &L2g[k]);
+        cp_async_commit();
         for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
     }
     const int W2 = (deg2 + 63) >> 6;
     const bool l2s = deg2 * W2 <= kL2Cap;
-    if constexpr (KW != 1) {
-        if (l2s)
-            for (int k = lane; k < deg2 * W2; k += 32) sL2[k] = L2g[k];
-    }
     // the b's of the row, ascending
 #pragma unroll
     for (int w = 0; w < KW; w++) {
@@ -1257,6 +1259,7 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         }
         smap[c] = (lo2 < deg2 && sN2[lo2] == x) ? (uint16_t)lo2 : (uint16_t)0xffff;
     }
+    if constexpr (KW != 1) cp_async_wait<0>();
     __syncwarp();
     const float e12x = sb[a].x - B1.x, e12y = sb[a].y - B1.y, e12z = sb[a].z - B1.z;
     const float4 b2 = sb[a];
