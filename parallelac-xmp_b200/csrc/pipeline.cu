@@ -1072,10 +1072,10 @@ struct EnumSmem;
 // balls of at most 64 upper neighbours: one link word per row, all staged
 template <>
 struct EnumSmem<1> {
-    static constexpr int kDeg = 64, kL2Cap = 64, kWarps = 8, kBufs = 2;
+    static constexpr int kDeg = 64, kL2Cap = 64, kWarps = 8, kBufs = 2, kLBufs = 2;
     float4 sb[kWarps][kDeg];      // balls of p's upper neighbours
     uint64_t sL[kWarps][kDeg];    // p's link rows
-    uint64_t sL2[kWarps][kBufs][kL2Cap]; // v2's link rows (when they fit), this row and the next
+    uint64_t sL2[kWarps][kLBufs][kL2Cap]; // v2's link rows (when they fit), this row and the next
     uint32_t sN2[kWarps][kBufs][kMaxDeg];// v2's upper neighbours, this row and the next
     uint64_t sE2[kWarps][kDeg];   // per neighbour v2: its first upper neighbour's index,
     uint64_t sLo[kWarps][kDeg];   // its link rows' offset,
@@ -1091,10 +1091,10 @@ struct EnumSmem<1> {
 // larger balls: rows read in place, v2's rows staged when they fit
 template <>
 struct EnumSmem<kMaxW> {
-    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kWarps = 4, kBufs = 1;
+    static constexpr int kDeg = kMaxDeg, kL2Cap = 256, kWarps = 4, kBufs = 2, kLBufs = 1;
     float4 sb[kWarps][kDeg];
-    uint64_t sL2[kWarps][kBufs][kL2Cap];
-    uint32_t sN2[kWarps][kBufs][kMaxDeg];
+    uint64_t sL2[kWarps][kLBufs][kL2Cap];  // this row's only
+    uint32_t sN2[kWarps][kBufs][kMaxDeg];  // this row and the next
     uint32_t sN[kWarps][kDeg];
     uint16_t smap[kWarps][kDeg];
     uint64_t pm[kWarps][32][kMaxW];
@@ -1178,13 +1178,34 @@ __device__ __forceinline__ void row_fetch(const TetArgs &A, EnumSmem<1> &S, int 
     cp_async_commit();
 }
 
+// A heavy row's v2: where its upper neighbours and link rows start, and
+// how many (KW = kMaxW; the light kernel stages these per ball).
+struct RowSrc {
+    uint64_t e2, loff;
+    int deg2;
+    bool valid;
+};
+__device__ __forceinline__ RowSrc row_src(const TetArgs &A, uint32_t v2) {
+    const uint64_t e2 = A.eoff[v2];
+    return RowSrc{e2, A.loff[v2], (int)(A.eoff[v2 + 1] - e2), true};
+}
+// Starts copying a heavy row's v2 neighbours into buffer buf (one cp.async
+// group of this thread, empty when there is no such row).
+__device__ __forceinline__ void heavy_fetch_n2(const TetArgs &A, EnumSmem<kMaxW> &S, int wib,
+                                               const RowSrc &r, int buf) {
+    const int lane = threadIdx.x & 31;
+    if (r.valid)
+        for (int k = lane; k < r.deg2; k += 32) cp_async4(&S.sN2[wib][buf][k], &A.ER[r.e2 + k]);
+    cp_async_commit();
+}
+
 // One row a of ball p: v2 = N[a].  N, sb, sCell hold p's upper neighbours,
 // their balls and cells (shared memory); L its link rows (W words each,
 // shared or global); the rest is per-warp scratch.
 template <int V, int KW>
 __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, EnumSmem<KW> &S,
                                         const int wib, QRes &qr, uint32_t p, int a, int buf,
-                                        int deg, int W,
+                                        const RowSrc &cur, const RowSrc &nxt, int deg, int W,
                                         const uint64_t *L, const Ball B1, const MolGrid &G,
                                         bool refute, unsigned long long &cand_acc,
                                         unsigned long long &alpha_acc, unsigned long long &kill_acc,
@@ -1201,10 +1222,29 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         ra[w] = w < W ? L[(uint64_t)a * W + w] : 0ull;
         nb += __popcll(ra[w]);
     }
-    if (nb < 2) return;
+    if constexpr (KW != 1) {
+        // heavy rows in a pipeline of cp.async groups: this row's
+        // neighbours (issued with the row before), its link rows (now), the
+        // next row's neighbours (after the search below); every path
+        // leaves exactly the next row's group pending
+        const int W2c = (cur.deg2 + 63) >> 6;
+        if (nb >= 2 && cur.deg2 * W2c <= EnumSmem<KW>::kL2Cap)
+            for (int k = lane; k < cur.deg2 * W2c; k += 32)
+                cp_async8(&S.sL2[wib][0][k], &A.link[cur.loff + k]);
+        cp_async_commit();
+        cp_async_wait<1>();  // this row's neighbours
+        __syncwarp();
+        if (nb < 2) {
+            if constexpr (KW == kMaxW) heavy_fetch_n2(A, S, wib, nxt, buf ^ 1);
+            cp_async_wait<1>();
+            return;
+        }
+    } else {
+        if (nb < 2) return;
+    }
     const uint32_t v2 = N[a];
     uint32_t *sN2 = S.sN2[wib][buf];
-    uint64_t *sL2 = S.sL2[wib][buf];
+    uint64_t *sL2 = S.sL2[wib][KW == 1 ? buf : 0];
     uint16_t *smap = S.smap[wib];
     uint8_t *sBl = S.sBl[wib];
     int deg2;
@@ -1214,16 +1254,8 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         deg2 = S.sD2[wib][a];
         L2g = A.link + S.sLo[wib][a];
     } else {
-        const uint64_t e2 = A.eoff[v2];
-        deg2 = (int)(A.eoff[v2 + 1] - e2);
-        L2g = A.link + A.loff[v2];
-        // v2's link rows arrive (cp.async) while its neighbours are staged
-        // and searched below
-        const int W2h = (deg2 + 63) >> 6;
-        if (deg2 * W2h <= kL2Cap)
-            for (int k = lane; k < deg2 * W2h; k += 32) cp_async8(&sL2[k], &L2g[k]);
-        cp_async_commit();
-        for (int k = lane; k < deg2; k += 32) sN2[k] = __ldg(&A.ER[e2 + k]);
+        deg2 = cur.deg2;
+        L2g = A.link + cur.loff;
     }
     const int W2 = (deg2 + 63) >> 6;
     const bool l2s = deg2 * W2 <= kL2Cap;
@@ -1259,7 +1291,10 @@ __device__ __forceinline__ void tet_row(const TetArgs &A, const TetQueue &Q, Enu
         }
         smap[c] = (lo2 < deg2 && sN2[lo2] == x) ? (uint16_t)lo2 : (uint16_t)0xffff;
     }
-    if constexpr (KW != 1) cp_async_wait<0>();
+    if constexpr (KW == kMaxW) {
+        heavy_fetch_n2(A, S, wib, nxt, buf ^ 1);
+        cp_async_wait<1>();  // this row's link rows
+    }
     __syncwarp();
     const float e12x = sb[a].x - B1.x, e12y = sb[a].y - B1.y, e12z = sb[a].z - B1.z;
     const float4 b2 = sb[a];
@@ -1497,16 +1532,30 @@ __global__ void __launch_bounds__(EnumSmem<KW>::kWarps * 32, KW == 1 ? 3 : 4)
                     cp_async_wait<0>();
                 }
                 __syncwarp();
-                tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, buf, deg, W, S.sL[wib], B1, G,
-                               refute, cand_acc, alpha_acc, kill_acc, ktest_acc, tally);
+                tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, buf, RowSrc{}, RowSrc{}, deg, W,
+                               S.sL[wib], B1, G, refute, cand_acc, alpha_acc, kill_acc, ktest_acc,
+                               tally);
                 __syncwarp();
                 buf ^= 1;
             }
         } else {
             const int a1 = min(a0 + A.unit_rows, deg - 2);
-            for (int a = a0; a < a1; a++)
-                tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, 0, deg, W, Lg, B1, G, refute,
-                               cand_acc, alpha_acc, kill_acc, ktest_acc, tally);
+            if constexpr (KW == kMaxW) {
+                // each row's v2 neighbours fetched while the row before
+                // is worked on (tet_row keeps the cp.async pipeline)
+                RowSrc cur = a0 < a1 ? row_src(A, S.sN[wib][a0]) : RowSrc{};
+                int buf = 0;
+                heavy_fetch_n2(A, S, wib, cur, buf);
+                for (int a = a0; a < a1; a++) {
+                    const RowSrc nxt = a + 1 < a1 ? row_src(A, S.sN[wib][a + 1]) : RowSrc{};
+                    tet_row<V, KW>(A, Q, S, wib, qr, (uint32_t)p, a, buf, cur, nxt, deg, W, Lg,
+                                   B1, G, refute, cand_acc, alpha_acc, kill_acc, ktest_acc, tally);
+                    cur = nxt;
+                    buf ^= 1;
+                }
+                cp_async_wait<0>();
+                __syncwarp();
+            }
         }
         __syncwarp();
     }
