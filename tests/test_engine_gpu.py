@@ -330,7 +330,7 @@ def test_verbose_reports_chunks_and_stages(pac, capfd):
 
 @pytest.mark.slow
 def test_assembly_2p5m_matches_restatement_digest(pac):
-    """The north star's large single pass: 2.5M balls (400 globules of 6,250
+    """The large single pass: 2.5M balls (400 globules of 6,250
     in an 8 x 10 x 5 grid at 60 A pitch), sol 1.4, alpha 1, as written, in
     one call (the tetrahedron queue runs in chunks); lists and stage counts
     against the restatement's digests (tests/golden/make_assembly_digest.py)."""
