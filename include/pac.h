@@ -120,7 +120,7 @@ typedef struct {
        balls with at most 64 upper neighbours (default 4), [1] of the
        orthosphere scan (4), [2] of the enumeration of larger balls (4),
        [3] rows of a large ball per work unit (8), [4] queue entries a scan
-       warp claims (512).
+       warp claims (256).
        reserved_i[5] = 1: no early refutation in the enumeration (every
        alpha tetrahedron goes to the scan; same lists).
        reserved_i[6] = 1: verify mode -- the scan also replays the

@@ -115,9 +115,9 @@ __global__ void k_check_finite(const float4 *b, uint64_t n, int *bad) {
 // scan warp claims at a time.  The first is the default.  None of them
 // changes the output.
 constexpr pac::LaunchShape kShapes[] = {
-    {4, 4, 4, 8, 512},  {3, 4, 4, 8, 512}, {2, 4, 4, 8, 512},  {4, 3, 4, 8, 512},
-    {4, 4, 3, 8, 512},  {4, 4, 6, 8, 512}, {4, 4, 4, 4, 512},  {4, 4, 4, 16, 512},
-    {4, 4, 4, 8, 128},  {4, 4, 4, 8, 2048}, {2, 2, 2, 8, 512}, {4, 2, 4, 4, 512}};
+    {4, 4, 4, 8, 256},  {3, 4, 4, 8, 256}, {2, 4, 4, 8, 256},  {4, 3, 4, 8, 256},
+    {4, 4, 3, 8, 256},  {4, 4, 6, 8, 256}, {4, 4, 4, 4, 256},  {4, 4, 4, 16, 256},
+    {4, 4, 4, 8, 512},  {4, 4, 4, 8, 2048}, {2, 2, 2, 8, 256}, {4, 2, 4, 4, 256}};
 constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
 static_assert(kNumShapes <= 16, "Tuner holds 16 timings");
 
