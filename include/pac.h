@@ -185,6 +185,10 @@ typedef struct {
     uint64_t filter_evals;    /* exact-mode: filtered decisions */
     uint64_t ortho_out_of_grid; /* window centres outside the grid */
     uint64_t max_degree;
+    /* stage times (CUDA events).  The host entry points copy each list to
+       host memory as soon as it is emitted, on a second stream, while the
+       later stages run: ms_d2h is the part of those copies that was left
+       after the last kernel. */
     double ms_total, ms_h2d, ms_grid, ms_edges, ms_tris, ms_tets, ms_tri_attach,
         ms_edge_attach, ms_emit, ms_d2h;
     uint64_t bytes_model; /* algorithmic bytes of the pass */

@@ -29,6 +29,50 @@ int set_error(int status, const std::string &msg) {
     return status;
 }
 
+int list_to_host_async(Ctx &c, int which, const uint32_t *src, size_t count, uint32_t **dst) {
+    *dst = nullptr;
+    if (!c.copy_stream) {
+        if (cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            c.copy_stream = nullptr;
+            return set_error(PAC_ERR_CUDA, "cudaStreamCreate (copy stream) failed");
+        }
+        for (auto &ev : c.copy_ev)
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+                return set_error(PAC_ERR_CUDA, "cudaEventCreate (copy stream) failed");
+    }
+    if (count == 0) return PAC_OK;
+    const size_t need = sizeof(uint32_t) * count;
+    if (need > c.pinned_size[which]) {
+        // nothing may still be copying into the old region
+        cudaStreamSynchronize(c.copy_stream);
+        if (c.pinned[which]) cudaFreeHost(c.pinned[which]);
+        c.pinned[which] = nullptr;
+        c.pinned_size[which] = 0;
+        const size_t sz = std::max(need + need / 4, size_t(1) << 20);
+        if (cudaMallocHost(&c.pinned[which], sz) != cudaSuccess) {
+            c.pinned[which] = nullptr;
+            cudaGetLastError();
+            return set_error(PAC_ERR_OOM, "cudaMallocHost for the output lists failed");
+        }
+        c.pinned_size[which] = sz;
+    }
+    cudaError_t e = cudaEventRecord(c.copy_ev[which], c.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c.copy_stream, c.copy_ev[which], 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.pinned[which], src, need, cudaMemcpyDeviceToHost, c.copy_stream);
+    if (e != cudaSuccess) return set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    *dst = static_cast<uint32_t *>(c.pinned[which]);
+    return PAC_OK;
+}
+
+int copies_join(Ctx &c) {
+    if (!c.copy_stream) return PAC_OK;
+    cudaError_t e = cudaEventRecord(c.copy_ev[3], c.copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c.stream, c.copy_ev[3], 0);
+    if (e != cudaSuccess) return set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    return PAC_OK;
+}
+
 Arena::~Arena() {
     for (auto &b : blocks_) cudaFree(b.base);
 }
@@ -102,6 +146,20 @@ size_t Arena::reserved() const {
 // ----------------------------------------------------------------- helpers
 namespace {
 
+// Timing events of one host entry point call, destroyed on every return path.
+struct EventSet {
+    cudaEvent_t e[3]{};
+    EventSet() {
+        for (auto &x : e) cudaEventCreate(&x);
+    }
+    ~EventSet() {
+        for (auto &x : e)
+            if (x) cudaEventDestroy(x);
+    }
+    EventSet(const EventSet &) = delete;
+    EventSet &operator=(const EventSet &) = delete;
+};
+
 __global__ void k_check_finite(const float4 *b, uint64_t n, int *bad) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -121,8 +179,11 @@ constexpr pac::LaunchShape kShapes[] = {
 constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
 static_assert(kNumShapes <= 16, "Tuner holds 16 timings");
 
+// One pass; with to_host the lists are copied into the context's pinned
+// host memory while the pass runs (out.h_*), complete on return.
 int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
-        const uint64_t *h_off, float sol, float alpha, pac::PassOutput &out, pac_stats *st) {
+        const uint64_t *h_off, float sol, float alpha, pac::PassOutput &out, pac_stats *st,
+        bool to_host = false) {
     pac::Ctx &c = ctx->c;
     if (!std::isfinite(sol) || !std::isfinite(alpha))
         return pac::set_error(PAC_ERR_INVALID_ARG, "sol_rad and alpha must be finite");
@@ -174,9 +235,13 @@ int run(pac_ctx *ctx, const float4 *d_balls, uint64_t n, uint32_t n_mol,
     pac_stats local;
     pac_stats *sp = st ? st : &local;
     pac::PassInput in{d_balls, n, n_mol, h_off, sol, alpha};
+    in.to_host = to_host;
     int rc = (c.opt.predicates == PAC_PRED_REFCOMPAT_FMA)
                  ? pac_fma::run_pass(c, cfg, in, out, sp)
                  : pac_strict::run_pass(c, cfg, in, out, sp);
+    // a pass that stopped early may have list copies in flight: they end
+    // before the pool or the pinned regions are reused
+    if (rc != PAC_OK && c.copy_stream) cudaStreamSynchronize(c.copy_stream);
     if (rc == PAC_OK && cand >= 0 && c.tuner.best < 0) {
         // every candidate gives the same lists; keep the fastest tetrahedron
         // stage once each has run on this context's work
@@ -206,41 +271,6 @@ int validate_opts(const pac_options &o) {
         return pac::set_error(PAC_ERR_INVALID_ARG, "unknown predicate mode");
     if (o.order != PAC_ORDER_REFERENCE && o.order != PAC_ORDER_CANONICAL)
         return pac::set_error(PAC_ERR_INVALID_ARG, "unknown order");
-    return PAC_OK;
-}
-
-// Copies the three device lists into the context's pinned buffer (grown if
-// needed) and points the outputs at it.
-int lists_to_host(pac::Ctx &c, const pac::PassOutput &po, uint32_t **e, uint32_t **t,
-                  uint32_t **q) {
-    size_t ne = 2 * po.n_edges, nt = 3 * po.n_tris, nq = 4 * po.n_tets;
-    size_t need = sizeof(uint32_t) * (ne + nt + nq);
-    if (need > c.pinned_size) {
-        if (c.pinned) cudaFreeHost(c.pinned);
-        c.pinned = nullptr;
-        c.pinned_size = 0;
-        size_t sz = std::max(need + need / 4, size_t(1) << 20);
-        if (cudaMallocHost(&c.pinned, sz) != cudaSuccess) {
-            cudaGetLastError();
-            return pac::set_error(PAC_ERR_OOM, "cudaMallocHost for the output lists failed");
-        }
-        c.pinned_size = sz;
-    }
-    uint32_t *base = static_cast<uint32_t *>(c.pinned);
-    *e = ne ? base : nullptr;
-    *t = nt ? base + ne : nullptr;
-    *q = nq ? base + ne + nt : nullptr;
-    cudaError_t err = cudaSuccess;
-    if (ne && err == cudaSuccess)
-        err = cudaMemcpyAsync(base, po.d_edges, sizeof(uint32_t) * ne, cudaMemcpyDeviceToHost, c.stream);
-    if (nt && err == cudaSuccess)
-        err = cudaMemcpyAsync(base + ne, po.d_tris, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost,
-                              c.stream);
-    if (nq && err == cudaSuccess)
-        err = cudaMemcpyAsync(base + ne + nt, po.d_tets, sizeof(uint32_t) * nq,
-                              cudaMemcpyDeviceToHost, c.stream);
-    if (err != cudaSuccess)
-        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(err));
     return PAC_OK;
 }
 
@@ -321,7 +351,14 @@ int pac_destroy(pac_ctx *ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     for (auto &ev : ctx->c.ev)
         if (ev) cudaEventDestroy(ev);
-    if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
+    if (ctx->c.copy_stream) {
+        cudaStreamSynchronize(ctx->c.copy_stream);
+        for (auto &ev : ctx->c.copy_ev)
+            if (ev) cudaEventDestroy(ev);
+        cudaStreamDestroy(ctx->c.copy_stream);
+    }
+    for (void *p : ctx->c.pinned)
+        if (p) cudaFreeHost(p);
     cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return PAC_OK;
@@ -380,56 +417,43 @@ int pac_alpha_complex(pac_ctx *ctx, const pac_ball *balls, uint32_t n, float sol
     cudaSetDevice(c.device);
     c.arena.reset();
     c.launches = 0;
-    cudaEvent_t e0, e1, e2, e3;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
-    cudaEventCreate(&e3);
-    cudaEventRecord(e0, c.stream);
+    EventSet ev;
+    cudaEventRecord(ev.e[0], c.stream);
     float4 *d = c.arena.alloc_n<float4>(n);
     if (!d) return PAC_ERR_OOM;
     cudaError_t e = cudaMemcpyAsync(d, balls, sizeof(float4) * n, cudaMemcpyHostToDevice, c.stream);
     if (e != cudaSuccess)
         return pac::set_error(PAC_ERR_CUDA, std::string("H2D: ") + cudaGetErrorString(e));
-    cudaEventRecord(e1, c.stream);
+    cudaEventRecord(ev.e[1], c.stream);
     uint64_t off[2] = {0, n};
     pac::PassOutput po;
-    int rc = run(ctx, d, n, 1, off, sol_rad, alpha, po, st);
+    // the lists reach the context's pinned memory during the pass
+    int rc = run(ctx, d, n, 1, off, sol_rad, alpha, po, st, true);
     if (rc) return rc;
-    cudaEventRecord(e2, c.stream);
+    cudaEventRecord(ev.e[2], c.stream);
+    e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess)
+        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
     out->n_edges = po.n_edges;
     out->n_tris = po.n_tris;
     out->n_tets = po.n_tets;
     out->on_device = 3;  // context-owned pinned host memory
-    if ((rc = lists_to_host(c, po, &out->edges, &out->tris, &out->tets))) {
-        pac_free_complex(out);
-        return rc;
-    }
-    cudaEventRecord(e3, c.stream);
-    e = cudaStreamSynchronize(c.stream);
-    if (e != cudaSuccess) {
-        pac_free_complex(out);
-        return pac::set_error(PAC_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
-    }
+    out->edges = po.h_edges;
+    out->tris = po.h_tris;
+    out->tets = po.h_tets;
     if (c.opt.order == PAC_ORDER_CANONICAL) {
         canonicalise<2>(out->edges, out->n_edges);
         canonicalise<3>(out->tris, out->n_tris);
         canonicalise<4>(out->tets, out->n_tets);
     }
     if (st) {
-        float a = 0, b = 0, t = 0;
-        cudaEventElapsedTime(&a, e0, e1);
-        cudaEventElapsedTime(&b, e2, e3);
-        cudaEventElapsedTime(&t, e0, e3);
-        st->ms_h2d = a;
-        st->ms_d2h = b;
+        float a = 0, t = 0;
+        cudaEventElapsedTime(&a, ev.e[0], ev.e[1]);
+        cudaEventElapsedTime(&t, ev.e[0], ev.e[2]);
+        st->ms_h2d = a;  // ms_d2h: set by the pass
         st->ms_total = t;
         st->kernels_launched = (uint32_t)c.launches;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
-    cudaEventDestroy(e3);
     return PAC_OK;
 }
 
@@ -472,25 +496,27 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
     cudaSetDevice(c.device);
     c.arena.reset();
     c.launches = 0;
-    cudaEvent_t e0, e3;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e3);
-    cudaEventRecord(e0, c.stream);
+    EventSet ev;
+    cudaEventRecord(ev.e[0], c.stream);
     float4 *d = c.arena.alloc_n<float4>(n);
-    if (!d) return PAC_ERR_OOM;
+    if (!d) {
+        pac_free_batch_complex(out);
+        return PAC_ERR_OOM;
+    }
     cudaMemcpyAsync(d, balls, sizeof(float4) * n, cudaMemcpyHostToDevice, c.stream);
+    cudaEventRecord(ev.e[1], c.stream);
     pac::PassOutput po;
-    int rc = run(ctx, d, n, (uint32_t)keep.size(), koff.data(), sol_rad, alpha, po, st);
+    // the lists reach the context's pinned memory during the pass
+    int rc = run(ctx, d, n, (uint32_t)keep.size(), koff.data(), sol_rad, alpha, po, st, true);
     if (rc) {
         pac_free_batch_complex(out);
         return rc;
     }
     out->on_device = 3;
-    if ((rc = lists_to_host(c, po, &out->edges, &out->tris, &out->tets))) {
-        pac_free_batch_complex(out);
-        return rc;
-    }
-    cudaEventRecord(e3, c.stream);
+    out->edges = po.h_edges;
+    out->tris = po.h_tris;
+    out->tets = po.h_tets;
+    cudaEventRecord(ev.e[2], c.stream);
     cudaError_t e = cudaStreamSynchronize(c.stream);
     if (e != cudaSuccess) {
         pac_free_batch_complex(out);
@@ -511,13 +537,13 @@ int pac_alpha_complex_batch(pac_ctx *ctx, const pac_ball *balls, const uint64_t 
             canonicalise<4>(out->tets + 4 * out->tet_off[m], out->tet_off[m + 1] - out->tet_off[m]);
         }
     if (st) {
-        float t = 0;
-        cudaEventElapsedTime(&t, e0, e3);
+        float a = 0, t = 0;
+        cudaEventElapsedTime(&a, ev.e[0], ev.e[1]);
+        cudaEventElapsedTime(&t, ev.e[0], ev.e[2]);
+        st->ms_h2d = a;  // ms_d2h: set by the pass
         st->ms_total = t;
         st->kernels_launched = (uint32_t)c.launches;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e3);
     return PAC_OK;
 }
 

@@ -89,6 +89,9 @@ struct PassInput {
     uint32_t n_mol;             // molecules
     const uint64_t *h_offsets;  // n_mol + 1 (host)
     float sol, alpha;
+    // copy each list into the context's pinned host memory as soon as it is
+    // emitted (on the copy stream, while the later stages run)
+    bool to_host = false;
 };
 
 // Device-resident result of a pass: lists in reference order with
@@ -97,6 +100,8 @@ struct PassOutput {
     uint32_t *d_edges = nullptr, *d_tris = nullptr, *d_tets = nullptr;
     uint64_t n_edges = 0, n_tris = 0, n_tets = 0;
     std::vector<uint64_t> edge_off, tri_off, tet_off;  // n_mol + 1 (host)
+    // PassInput::to_host: the lists in the context's pinned host memory
+    uint32_t *h_edges = nullptr, *h_tris = nullptr, *h_tets = nullptr;
 };
 
 struct Ctx {
@@ -106,10 +111,15 @@ struct Ctx {
     pac_options opt{};
     cudaEvent_t ev[16]{};
     int launches = 0;
-    // pinned host memory for the lists returned by the host entry points;
-    // grows, never shrinks, reused by every call
-    void *pinned = nullptr;
-    size_t pinned_size = 0;
+    // pinned host memory for the lists returned by the host entry points,
+    // one region per list (edges, triangles, tetrahedra); each grows, never
+    // shrinks, and is reused by every call
+    void *pinned[3] = {nullptr, nullptr, nullptr};
+    size_t pinned_size[3] = {0, 0, 0};
+    // device-to-host copies of the lists run on their own stream, so that a
+    // list emitted early crosses PCIe while the later stages compute
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev[4]{};
     // bytes for the alpha-tetrahedron queue, fixed at the context's first
     // pass (a quarter of the memory free then, at most 12 GiB), so that later
     // passes lay out the pool the same way
@@ -121,6 +131,15 @@ int union_measure_device(Ctx &ctx, const double4 *d_balls, uint32_t n, const uin
                          uint64_t ne, const uint32_t *d_tris, uint64_t nt, const uint32_t *d_tets,
                          uint64_t nq, double *vol, double *area, double *d_dV, double *d_dA,
                          float *ms);
+
+// Starts copying count words of the device list src into the context's
+// pinned region `which` (0 edges, 1 triangles, 2 tetrahedra) on the copy
+// stream, after the work queued so far on the context's stream; *dst gets
+// the host address (nullptr when count is 0).  The copy is complete once
+// copies_join's wait has passed on the context's stream.
+int list_to_host_async(Ctx &c, int which, const uint32_t *src, size_t count, uint32_t **dst);
+// Makes the context's stream wait for every copy started so far.
+int copies_join(Ctx &c);
 
 // Sets the thread-local error detail; returns status.
 int set_error(int status, const std::string &msg);

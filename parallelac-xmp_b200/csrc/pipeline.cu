@@ -2667,53 +2667,10 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
     }
     tm.mark();  // 4
 
-    // ---- final triangles and edges
-    uint32_t *tricount = ar.alloc_n<uint32_t>(n);
-    uint64_t *tpos = ar.alloc_n<uint64_t>(n + 1);
-    uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
-    if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
-    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
-    if (cfg.slab_world > 1) CK(cudaMemsetAsync(tricount, 0, sizeof(uint32_t) * n, s));
-    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(own_hi - work_lo), 148 * 4), 256, 0, s>>>(
-        work_lo, own_hi, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids,
-        in.alpha, ctr);
-    LAUNCH_CHECK(ctx);
-    tm.mark();  // 5
-    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
-    k_edge_final<V><<<std::min<unsigned>(warp_blocks(own_hi - own_lo), 148 * 5), 256, 0, s>>>(
-        own_lo, own_hi, at, eoff, ER, eflag, cellbeg, mol, grids, ctr);
-    LAUNCH_CHECK(ctx);
-    if (cfg.slab_world > 1) {
-        // only the owned balls' triangles and edges are output
-        if (own_lo > work_lo)
-            CK(cudaMemsetAsync(tricount + work_lo, 0, sizeof(uint32_t) * (own_lo - work_lo), s));
-        uint64_t eb[2] = {0, 0};
-        CK(cudaMemcpyAsync(&eb[0], eoff + own_lo, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&eb[1], eoff + own_hi, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        if (eb[0]) CK(cudaMemsetAsync(eflag, 0, eb[0], s));
-        if (nE > eb[1]) CK(cudaMemsetAsync(eflag + eb[1], 0, nE - eb[1], s));
-    }
-    tm.mark();  // 6
-
-    // ---- emission
-    rc = exclusive_scan(ctx, tricount, n, tpos);
-    if (rc) return rc;
-    rc = exclusive_scan(ctx, eflag, nE, epos);
-    if (rc) return rc;
-    uint64_t nT = 0, nEf = 0;
-    CK(cudaMemcpyAsync(&nT, tpos + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(&nEf, epos + nE, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    out.d_edges = ar.alloc_n<uint32_t>(2 * nEf);
-    out.d_tris = ar.alloc_n<uint32_t>(3 * nT);
+    // ---- emission of the tetrahedra: final now, so with to_host their copy
+    // crosses PCIe while the triangles and edges are decided
     out.d_tets = ar.alloc_n<uint32_t>(4 * nQ);
-    if (!out.d_edges || !out.d_tris || !out.d_tets) return PAC_ERR_OOM;
-    k_emit_edges<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, ER, eflag, epos, orig, out.d_edges);
-    LAUNCH_CHECK(ctx);
-    k_emit_tris<<<warp_blocks(own_hi - own_lo), 256, 0, s>>>(own_lo, own_hi, eoff, ER, loff, faces,
-                                                            tpos, orig, out.d_tris);
-    LAUNCH_CHECK(ctx);
+    if (!out.d_tets) return PAC_ERR_OOM;
     if (cfg.tet_mode == PAC_TETS_AS_RUN) {
         CK(cudaMemcpyAsync(out.d_tets, tets_sorted, sizeof(uint32_t) * 4 * (nQ ? nQ : 1),
                            cudaMemcpyDeviceToDevice, s));
@@ -2731,6 +2688,65 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                                                            out.d_tets);
         LAUNCH_CHECK(ctx);
     }
+    if (in.to_host && (rc = pac::list_to_host_async(ctx, 2, out.d_tets, 4 * nQ, &out.h_tets)))
+        return rc;
+    tm.mark();  // 5
+
+    // ---- final triangles
+    uint32_t *tricount = ar.alloc_n<uint32_t>(n);
+    uint64_t *tpos = ar.alloc_n<uint64_t>(n + 1);
+    uint64_t *epos = ar.alloc_n<uint64_t>(nE + 1);
+    if (!tricount || !tpos || !epos) return PAC_ERR_OOM;
+    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+    if (cfg.slab_world > 1) CK(cudaMemsetAsync(tricount, 0, sizeof(uint32_t) * n, s));
+    k_tri_attach<V><<<std::min<unsigned>(warp_blocks(own_hi - work_lo), 148 * 4), 256, 0, s>>>(
+        work_lo, own_hi, at, eoff, ER, loff, link, faces, tricount, eflag, cellbeg, mol, grids,
+        in.alpha, ctr);
+    LAUNCH_CHECK(ctx);
+    tm.mark();  // 6
+    // only the owned balls' triangles are output
+    if (cfg.slab_world > 1 && own_lo > work_lo)
+        CK(cudaMemsetAsync(tricount + work_lo, 0, sizeof(uint32_t) * (own_lo - work_lo), s));
+    rc = exclusive_scan(ctx, tricount, n, tpos);
+    if (rc) return rc;
+    uint64_t nT = 0;
+    CK(cudaMemcpyAsync(&nT, tpos + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    out.d_tris = ar.alloc_n<uint32_t>(3 * nT);
+    if (!out.d_tris) return PAC_ERR_OOM;
+    k_emit_tris<<<warp_blocks(own_hi - own_lo), 256, 0, s>>>(own_lo, own_hi, eoff, ER, loff, faces,
+                                                            tpos, orig, out.d_tris);
+    LAUNCH_CHECK(ctx);
+    if (in.to_host && (rc = pac::list_to_host_async(ctx, 1, out.d_tris, 3 * nT, &out.h_tris)))
+        return rc;
+    tm.mark();  // 7
+
+    // ---- final edges
+    CK(cudaMemsetAsync(ctr + C_NEXT, 0, sizeof(unsigned long long), s));
+    k_edge_final<V><<<std::min<unsigned>(warp_blocks(own_hi - own_lo), 148 * 5), 256, 0, s>>>(
+        own_lo, own_hi, at, eoff, ER, eflag, cellbeg, mol, grids, ctr);
+    LAUNCH_CHECK(ctx);
+    if (cfg.slab_world > 1) {
+        // only the owned balls' edges are output
+        uint64_t eb[2] = {0, 0};
+        CK(cudaMemcpyAsync(&eb[0], eoff + own_lo, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&eb[1], eoff + own_hi, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (eb[0]) CK(cudaMemsetAsync(eflag, 0, eb[0], s));
+        if (nE > eb[1]) CK(cudaMemsetAsync(eflag + eb[1], 0, nE - eb[1], s));
+    }
+    tm.mark();  // 8
+    rc = exclusive_scan(ctx, eflag, nE, epos);
+    if (rc) return rc;
+    uint64_t nEf = 0;
+    CK(cudaMemcpyAsync(&nEf, epos + nE, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    out.d_edges = ar.alloc_n<uint32_t>(2 * nEf);
+    if (!out.d_edges) return PAC_ERR_OOM;
+    k_emit_edges<<<blocks_for(n, 256), 256, 0, s>>>(n, eoff, ER, eflag, epos, orig, out.d_edges);
+    LAUNCH_CHECK(ctx);
+    if (in.to_host && (rc = pac::list_to_host_async(ctx, 0, out.d_edges, 2 * nEf, &out.h_edges)))
+        return rc;
     out.n_edges = nEf;
     out.n_tris = nT;
     out.n_tets = nQ;
@@ -2757,7 +2773,10 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
             out.tet_off[m] = h[2 * (nm + 1) + m];
         }
     }
-    tm.mark();  // 7
+    tm.mark();  // 9
+    // the lists' copies that did not finish under the later stages
+    if (in.to_host && (rc = pac::copies_join(ctx))) return rc;
+    tm.mark();  // 10
     unsigned long long hc[C_NCOUNTERS];
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -2790,9 +2809,10 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
         st->ms_edges = tm.ms(1, 2);
         st->ms_tris = tm.ms(2, 3);
         st->ms_tets = tm.ms(3, 4);
-        st->ms_tri_attach = tm.ms(4, 5);
-        st->ms_edge_attach = tm.ms(5, 6);
-        st->ms_emit = tm.ms(6, 7);
+        st->ms_tri_attach = tm.ms(5, 6);
+        st->ms_edge_attach = tm.ms(7, 8);
+        st->ms_emit = tm.ms(4, 5) + tm.ms(6, 7) + tm.ms(8, 9);
+        if (in.to_host) st->ms_d2h = tm.ms(9, 10);
         // the reference's data movement for this pass: balls in, lists out,
         // and every candidate list (edges 8 B, triangles 12 B + 16 B
         // orthosphere, tetrahedra 16 B + 16 B orthosphere) written and read
@@ -2812,7 +2832,7 @@ static int run_pass_v(pac::Ctx &ctx, const pac::PipelineConfig &cfg, const pac::
                      "[pac] %llu balls: grid %.3f, edges %.3f, triangles %.3f, tetrahedra %.3f, "
                      "triangle attachment %.3f, edge attachment %.3f, emission %.3f ms\n",
                      (unsigned long long)n, tm.ms(0, 1), tm.ms(1, 2), tm.ms(2, 3), tm.ms(3, 4),
-                     tm.ms(4, 5), tm.ms(5, 6), tm.ms(6, 7));
+                     tm.ms(5, 6), tm.ms(7, 8), tm.ms(4, 5) + tm.ms(6, 7) + tm.ms(8, 9));
     return PAC_OK;
 }
 
