@@ -141,20 +141,38 @@ def _check(status):
         raise PacError(status, _lib().pac_last_error().decode())
 
 
+_POOL = None
+_POOL_PID = None
+
+
+def _pool():
+    """The binding's copy threads, created on first use (and again in a
+    forked child, which does not inherit the parent's threads)."""
+    global _POOL, _POOL_PID
+    if _POOL is None or _POOL_PID != os.getpid():
+        _POOL = ThreadPoolExecutor(min(os.cpu_count() or 1, 64))
+        _POOL_PID = os.getpid()
+    return _POOL
+
+
 def _copy_many(srcs):
-    """Copies of several arrays, large ones in 32 MB slices spread over the
-    host's threads (numpy releases the GIL while copying; the first touch
-    of the new pages is most of the cost): lists of a batched pass run to
+    """Copies of several 1-D arrays.  Results of 4 MB and more are copied in
+    slices of 1-32 MB spread over the host's threads (numpy releases the GIL
+    while copying; the first touch of the new pages is most of the cost):
+    a 100k-ball complex is 27 MB of lists, a batched pass's run to
     gigabytes."""
-    outs = [np.empty_like(a) if a.nbytes >= (16 << 20) else a.copy() for a in srcs]
-    jobs = []
-    for a, o in zip(srcs, outs):
-        if a.nbytes >= (16 << 20):
-            step = max(1, (32 << 20) // a.itemsize)
-            jobs += [(a, o, i, min(len(a), i + step)) for i in range(0, len(a), step)]
-    if jobs:
-        with ThreadPoolExecutor(min(len(jobs), os.cpu_count() or 1, 64)) as ex:
-            list(ex.map(lambda j: np.copyto(j[1][j[2]:j[3]], j[0][j[2]:j[3]]), jobs))
+    threads = min(os.cpu_count() or 1, 64)
+    total = sum(a.nbytes for a in srcs)
+    if total < (4 << 20) or threads == 1:
+        return [a.copy() for a in srcs]
+    step_b = min(32 << 20, max(1 << 20, total // (2 * threads)))
+    outs, jobs = [], []
+    for a in srcs:
+        o = np.empty_like(a)
+        outs.append(o)
+        step = max(1, step_b // max(1, a.itemsize))
+        jobs += [(a, o, i, min(len(a), i + step)) for i in range(0, len(a), step)]
+    list(_pool().map(lambda j: np.copyto(j[1][j[2]:j[3]], j[0][j[2]:j[3]]), jobs))
     return outs
 
 
@@ -166,12 +184,6 @@ def _view(ptr, count, k):
     if count == 0:
         return np.zeros((0,), np.uint32)
     return np.ctypeslib.as_array(ptr, (count * k,))
-
-
-def _arr(ptr, count, k):
-    if count == 0:
-        return np.zeros((0, k), np.uint32)
-    return _copy(np.ctypeslib.as_array(ptr, (count * k,))).reshape(count, k)
 
 
 class Result:
@@ -254,8 +266,9 @@ class Engine:
             timing["c_call_s"] = time.perf_counter() - t0
         _check(rc)
         try:
-            return Result(_arr(cx.edges, cx.n_edges, 2), _arr(cx.tris, cx.n_tris, 3),
-                          _arr(cx.tets, cx.n_tets, 4), st.as_dict())
+            E, T, Q = _copy_many([_view(cx.edges, cx.n_edges, 2), _view(cx.tris, cx.n_tris, 3),
+                                  _view(cx.tets, cx.n_tets, 4)])
+            return Result(E.reshape(-1, 2), T.reshape(-1, 3), Q.reshape(-1, 4), st.as_dict())
         finally:
             _lib().pac_free_complex(ctypes.byref(cx))
 
