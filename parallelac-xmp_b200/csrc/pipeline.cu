@@ -1612,7 +1612,7 @@ constexpr int kScanRefill = 16;  // idle lanes that trigger a refill
 // arithmetic; A.verify replays every certified decision too and counts
 // disagreements (C_CERT_BAD).  Survivors are recorded and mark their faces.
 template <int V>
-__global__ void __launch_bounds__(256, 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
+__global__ void __launch_bounds__(256, V == pac::kExact ? 2 : 4) k_tets_scan(TetArgs A, TetQueue Q, uint64_t nq,
                                                       unsigned long long *claim) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1;
